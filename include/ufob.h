@@ -1,0 +1,243 @@
+/*
+ * ufob.h -- C ABI of the B200 filtered-backprojection engine.
+ *
+ * The engine replaces the GPU work of three ufo-filters tasks on the FBP path:
+ *   fft ! filter ! ifft   (the ramp-filter stage, fused into one kernel)
+ *   backproject           (parallel beam)
+ *   general-backproject   (parallel, cone and laminography)
+ * Each task keeps the reference's property names, types, ranges and defaults;
+ * the *_props structs below mirror the GObject properties field by field and
+ * ufob_*_set_property() accepts the reference's property names as strings, so
+ * a GObject plugin adapter can forward g_object_set() calls unchanged.
+ *
+ * Conventions
+ *  - Every function returns ufob_status; on failure ufob_last_error() returns a
+ *    thread-local message (the analogue of the reference's GError text).
+ *  - Pointers named d_* are device pointers owned by the caller; the engine
+ *    owns its plans, tables and workspaces and frees them in ufob_*_destroy().
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Work is enqueued asynchronously on it, like a task's in-order queue.
+ *  - A handle may be used from one host thread at a time.
+ *  - There is no CPU fallback: without a usable sm_100 device every run
+ *    function fails with UFOB_ERR_CUDA.
+ */
+#ifndef UFOB_H
+#define UFOB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UFOB_VERSION_MAJOR 0
+#define UFOB_VERSION_MINOR 1
+
+typedef enum {
+    UFOB_OK = 0,
+    UFOB_ERR_INVALID = 1,     /* bad argument or property value */
+    UFOB_ERR_SETUP = 2,       /* UFO_TASK_ERROR_SETUP in the reference */
+    UFOB_ERR_REQUISITION = 3, /* UFO_TASK_ERROR_GET_REQUISITION in the reference */
+    UFOB_ERR_CUDA = 4,        /* CUDA runtime / launch failure, or no device */
+    UFOB_ERR_NOMEM = 5,       /* device allocation failed */
+    UFOB_ERR_TIMEOUT = 6,     /* a bounded device-side wait ran out */
+    UFOB_ERR_UNSUPPORTED = 7  /* valid in the reference, not implemented here */
+} ufob_status;
+
+typedef enum {
+    UFOB_F32 = 0,
+    UFOB_F16 = 1,
+    UFOB_BF16 = 2,
+    UFOB_F64 = 3,
+    UFOB_U8 = 4,
+    UFOB_U16 = 5,
+    UFOB_U32 = 6
+} ufob_dtype;
+
+const char *ufob_last_error(void);
+const char *ufob_status_string(ufob_status status);
+/* Returns UFOB_OK when a CUDA device of compute capability 10.x is usable. */
+ufob_status ufob_device_check(int *cc_major, int *cc_minor, int *num_sms);
+/* Synchronises the current device and reports (then clears) the device error
+ * word that kernels with bounded waits set instead of trapping:
+ * UFOB_ERR_TIMEOUT if a wait gave up since the last call. */
+ufob_status ufob_device_status(void);
+
+/* ------------------------------------------------------------------ filter
+ * Fused `fft dimensions=1 [size-x] ! filter ! ifft dimensions=1 [crop-width]`.
+ * Replaces: src/ufo-fft-task.c:123-336 (spread, forward FFT),
+ *           src/ufo-filter-task.c:117-144,278-336 (coefficients, multiply),
+ *           src/ufo-ifft-task.c:111-177,287-311 (backward FFT, crop, 1/N).
+ */
+typedef enum {
+    UFOB_FILTER_RAMP = 0,          /* "ramp" */
+    UFOB_FILTER_RAMP_FROMREAL = 1, /* "ramp-fromreal" (default) */
+    UFOB_FILTER_BUTTERWORTH = 2,   /* "butterworth" */
+    UFOB_FILTER_FARIS_BYER = 3,    /* "faris-byer" */
+    UFOB_FILTER_HAMMING = 4,       /* "hamming" */
+    UFOB_FILTER_BH3 = 5            /* "bh3" */
+} ufob_filter_type;
+
+/* Layout of filtered output rows (engine extension, not a reference property). */
+typedef enum {
+    UFOB_LAYOUT_ROWS = 0,  /* [rows][crop_width] of the output dtype */
+    UFOB_LAYOUT_PAIRS = 1  /* [rows][pair_stride] 32-bit pairs (s[j-1], s[j]), F16/BF16 only;
+                              pair_stride = round_up(crop_width + 1, 4) */
+} ufob_layout;
+
+typedef struct {
+    int filter;         /* ufob_filter_type, property "filter"; default ramp-fromreal */
+    float cutoff;       /* "cutoff" [0,1], default 0.5 */
+    float order;        /* "order" [2,32], default 4 (Butterworth) */
+    float tau;          /* "tau", default 0.1 (Faris-Byer) */
+    float theta;        /* "theta", default 1.0 (Faris-Byer) */
+    float scale;        /* "scale", default 1.0 */
+    uint32_t size_x;    /* fft "size-x" [0,32768], 0 = input width */
+    uint32_t crop_width;/* ifft "crop-width" [0,32768], 0 = FFT width */
+} ufob_filter_props;
+
+typedef struct ufob_filter ufob_filter;
+
+void ufob_filter_props_init(ufob_filter_props *props);
+ufob_status ufob_filter_create(const ufob_filter_props *props, ufob_filter **out);
+ufob_status ufob_filter_set_property(ufob_filter *f, const char *name, double value);
+ufob_status ufob_filter_set_property_string(ufob_filter *f, const char *name, const char *value);
+/* Output size for an input of `width` x `height` (get_requisition). */
+ufob_status ufob_filter_get_requisition(ufob_filter *f, uint32_t width, uint32_t height,
+                                        uint32_t *out_width, uint32_t *out_height);
+/* Filter `rows` rows of `width` floats (row pitch in_pitch floats, 0 = width).
+ * out_dtype F32/F16/BF16, out_layout per ufob_layout, out_pitch in elements
+ * (0 = packed).  The interleaved coefficient vector the reference would upload
+ * is available through ufob_filter_coefficients(). */
+ufob_status ufob_filter_run(ufob_filter *f, const float *d_in, uint32_t width, uint32_t rows,
+                            uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
+                            uint32_t out_pitch, void *stream);
+/* Host copy of the 2*nfft interleaved coefficients for an input of `width`. */
+ufob_status ufob_filter_coefficients(ufob_filter *f, uint32_t width, float *host_out, uint32_t n);
+/* The reference `filter` task alone: multiply complex-interleaved rows
+ * [rows][2*nfft] element-wise by the coefficient vector (filter.cl:20-29). */
+ufob_status ufob_filter_apply_spectrum(ufob_filter *f, const float *d_in, float *d_out, uint32_t width2,
+                                       uint32_t rows, void *stream);
+void ufob_filter_destroy(ufob_filter *f);
+
+/* -------------------------------------------------------------- backproject
+ * Parallel-beam backprojection.  Replaces src/ufo-backproject-task.c:96-267
+ * and src/kernels/backproject.cl:24-94.
+ */
+typedef enum { UFOB_BP_NEAREST = 0, UFOB_BP_TEXTURE = 1 } ufob_bp_mode;
+
+typedef struct {
+    uint32_t num_projections; /* "num-projections", 0 = sinogram height */
+    uint32_t offset;          /* "offset": first LUT entry used */
+    double axis_pos;          /* "axis-pos", <= 0 means width / 2; default -1 */
+    double angle_step;        /* "angle-step", <= 0 means pi / num-projections */
+    double angle_offset;      /* "angle-offset" [rad] */
+    int mode;                 /* "mode": ufob_bp_mode, default texture (linear) */
+    uint32_t roi_x, roi_y;    /* "roi-x", "roi-y" */
+    uint32_t roi_width;       /* "roi-width", 0 = sinogram width */
+    uint32_t roi_height;      /* "roi-height", 0 = sinogram width */
+    /* engine extensions */
+    int compensated;          /* blocked Kahan over angle blocks: 0 off, 1 on, -1 auto (>=1500 angles
+                                 when the sinogram is stored as F16/BF16) */
+    int tile;                 /* kernel shape id from the autotuner, -1 = automatic */
+} ufob_bp_props;
+
+typedef struct ufob_backproject ufob_backproject;
+
+void ufob_bp_props_init(ufob_bp_props *props);
+ufob_status ufob_backproject_create(const ufob_bp_props *props, ufob_backproject **out);
+ufob_status ufob_backproject_set_property(ufob_backproject *bp, const char *name, double value);
+ufob_status ufob_backproject_set_property_string(ufob_backproject *bp, const char *name, const char *value);
+ufob_status ufob_backproject_get_requisition(ufob_backproject *bp, uint32_t width, uint32_t height,
+                                             uint32_t *out_width, uint32_t *out_height);
+/* Backproject `nslices` sinograms of `height` rows x `width` bins.
+ * sino_dtype F32 with sino_layout ROWS (row pitch in floats, 0 = width), or
+ * F16/BF16 with layout PAIRS as written by ufob_filter_run (pitch in pairs).
+ * Sinogram z starts at d_sino + z * slice_pitch elements (0 = height * pitch).
+ * Output slice z is [roi_height][roi_width] floats at d_out + z * roi_w * roi_h. */
+ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_dtype sino_dtype,
+                                 ufob_layout sino_layout, uint32_t width, uint32_t height, uint32_t nslices,
+                                 uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream);
+void ufob_backproject_destroy(ufob_backproject *bp);
+
+/* ------------------------------------------------------------------- fbp
+ * Whole `fft ! filter ! ifft ! backproject` chain for a stack of sinograms
+ * [nslices][height][width] float32 -> [nslices][roi_h][roi_w] float32.
+ * `storage` is the filtered-sinogram storage type (F32, F16 or BF16).  The
+ * engine streams slice groups through its own workspace.  Host-pointer
+ * variant: inputs/outputs in host memory (pinned or pageable), copies are
+ * overlapped with compute on internal streams.
+ */
+typedef struct ufob_fbp ufob_fbp;
+ufob_status ufob_fbp_create(const ufob_filter_props *fprops, const ufob_bp_props *bprops, ufob_dtype storage,
+                            ufob_fbp **out);
+ufob_status ufob_fbp_run(ufob_fbp *fbp, const float *d_sino, uint32_t width, uint32_t height, uint32_t nslices,
+                         float *d_out, void *stream);
+ufob_status ufob_fbp_run_host(ufob_fbp *fbp, const float *h_sino, uint32_t width, uint32_t height,
+                              uint32_t nslices, float *h_out, uint32_t slices_per_chunk);
+/* Output size and the backprojection kernel time of the last run, if timed. */
+ufob_status ufob_fbp_get_requisition(ufob_fbp *fbp, uint32_t width, uint32_t height, uint32_t *out_width,
+                                     uint32_t *out_height);
+void ufob_fbp_destroy(ufob_fbp *fbp);
+
+/* ------------------------------------------------------ general-backproject
+ * Replaces src/ufo-general-backproject-task.c (setup :1411-1462,
+ * get_requisition :1464-1587, process :1610-1706, generate :1708-1764).
+ * Array-valued properties (the geometry, regions) are set with
+ * ufob_gbp_set_array(); a single value broadcasts to all projections.
+ */
+typedef struct ufob_gbp ufob_gbp;
+ufob_status ufob_gbp_create(ufob_gbp **out);
+ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double value);
+ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value);
+ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n);
+/* setup(): validates num-projections, gray mapping; builds angle tables. */
+ufob_status ufob_gbp_setup(ufob_gbp *g);
+/* Slice size and slice count for projections of width x height. */
+ufob_status ufob_gbp_get_requisition(ufob_gbp *g, uint32_t width, uint32_t height, uint32_t *out_width,
+                                     uint32_t *out_height, uint32_t *num_slices);
+/* Reconstruct from all num-projections projections at once:
+ * d_proj = [n][height][width] float32 (row pitch = width).  d_volume receives
+ * [num_slices][out_h][out_w] of the store-type.  Equivalent to process() for
+ * every projection followed by generate() for every slice. */
+ufob_status ufob_gbp_run(ufob_gbp *g, const float *d_proj, uint32_t width, uint32_t height, void *d_volume,
+                         void *stream);
+/* Streaming form of the reductor: push one projection (process()), then read
+ * slices out (generate()).  generate fails with UFOB_ERR_INVALID until all
+ * num-projections projections were pushed, as the reference refuses output. */
+ufob_status ufob_gbp_process(ufob_gbp *g, const float *d_projection, uint32_t width, uint32_t height,
+                             void *stream);
+ufob_status ufob_gbp_generate(ufob_gbp *g, void *d_slice, uint32_t index, void *stream);
+void ufob_gbp_destroy(ufob_gbp *g);
+
+/* ------------------------------------------------------------ batched jobs
+ * Uneven batch of parallel-beam reconstructions run by one persistent kernel
+ * over a device work queue (captured in a CUDA graph on first use).
+ */
+typedef struct {
+    const float *d_sino;  /* [height][width] float32 */
+    float *d_out;         /* [roi_height][roi_width] float32 */
+    uint32_t width, height;
+    double axis_pos;      /* <= 0: width / 2 */
+    double angle_step;    /* <= 0: pi / height */
+    double angle_offset;
+} ufob_job;
+
+typedef struct ufob_batch ufob_batch;
+ufob_status ufob_batch_create(const ufob_filter_props *fprops, ufob_dtype storage, ufob_batch **out);
+ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint32_t n, void *stream);
+void ufob_batch_destroy(ufob_batch *b);
+
+/* ------------------------------------------------------------- utilities */
+/* Analytic parallel-beam projection of ellipses (rows cx, cy, a, b, phi, rho
+ * in units where the reconstruction circle has radius 1) into [P][W] float
+ * sinograms in pixel-length units: used to synthesise inputs on the device. */
+ufob_status ufob_phantom_sinogram(const double *h_ellipses, uint32_t n_ellipses, uint32_t width,
+                                  uint32_t n_angles, double angle_step, double axis, double scale, float *d_sino,
+                                  void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UFOB_H */

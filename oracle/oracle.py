@@ -1,0 +1,377 @@
+"""CPU oracle for the filtered-backprojection path (TEST INFRASTRUCTURE ONLY).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module, and only as the checker.  The engine under
+``ufo-filters_b200/`` never calls it.
+
+It restates in NumPy/FP64 what the reference ufo-filters tasks compute:
+
+* ``filter_coefficients`` -- src/ufo-filter-task.c:162-336 (ramp, ramp-fromreal,
+  butterworth, faris-byer, hamming, bh3; mirroring; ramp-fromreal's FFT).
+* ``fft_filter_ifft`` -- the ``fft ! filter ! ifft`` chain:
+  src/ufo-fft-task.c:123-196,293-336 (spread/zero-pad to size-x),
+  src/kernels/filter.cl:20-29 (element-wise multiply of the interleaved floats),
+  src/ufo-ifft-task.c:111-177,287-311 (backward FFT, real part, crop, 1/N).
+* ``backproject`` -- src/ufo-backproject-task.c:96-150,174-267 and
+  src/kernels/backproject.cl:24-94 (via the C oracle).
+* ``general_backproject`` -- src/ufo-general-backproject-task.c (via the C oracle).
+
+The heavy loops live in ``ufob_oracle.c`` (built into ``liboracle.so`` by the
+Makefile next to this file).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+FILTERS = ["ramp", "ramp-fromreal", "butterworth", "faris-byer", "hamming", "bh3"]
+
+INTERP_EXACT, INTERP_TEX8, INTERP_NEAREST = 0, 1, 2
+ADDR_CLAMP, ADDR_CLAMP_TO_EDGE = 0, 1
+
+# geometry table columns (must match ufob_oracle.c)
+GEOM_COLS = [
+    "axis-angle-z", "axis-angle-x", "axis-angle-y",
+    "volume-angle-x", "volume-angle-y", "volume-angle-z",
+    "detector-angle-x", "detector-angle-y", "detector-angle-z",
+    "center-position-x", "center-position-z",
+    "source-position-x", "source-position-y", "source-position-z",
+    "detector-position-x", "detector-position-y", "detector-position-z",
+]
+F_WITH_AXIS, F_WITH_VOLUME, F_PERPENDICULAR = 1, 2, 4
+F_SHIFTED_DETECTOR, F_SHIFTED_SOURCE, F_PARALLEL = 8, 16, 32
+
+
+def lib():
+    """Load (building on first use) the C oracle."""
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        src = os.path.join(HERE, "ufob_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+        _LIB = ctypes.CDLL(path)
+        d, i, pf, pd = ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p
+        _LIB.oracle_bp_parallel.argtypes = [pf, i, i, i, pd, pd, i, d, i, i, i, i, i, pd]
+        _LIB.oracle_gbp.argtypes = [pf, i, i, i, pd, i, i, pd, d, d, d, d, d, i, i, i, d, i, i, pd]
+        _LIB.oracle_gbp_project_point.argtypes = [pd, i, d, d, d, pd, pd]
+        _LIB.oracle_gbp_project_point.restype = d
+        _LIB.oracle_forwardproject.argtypes = [pf, i, i, d, d, pd]
+        _LIB.oracle_ellipse_sinogram.argtypes = [pd, i, i, i, pd, d, d, pd]
+        _LIB.oracle_ellipse_image.argtypes = [pd, i, i, d, d, i, pd]
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+# --------------------------------------------------------------------------- filter
+
+def _mirror(f, width):
+    """src/ufo-filter-task.c:162-169"""
+    for k in range(width // 2 + 2, width, 2):
+        f[k] = f[width - k]
+        f[k + 1] = f[width - k + 1]
+
+
+def _padding_value(x):
+    """src/ufo-filter-task.c:242-252"""
+    padding, result = 2 * x, 1
+    while result < padding:
+        result *= 2
+    return result
+
+
+def filter_coefficients(nfft, filter="ramp-fromreal", cutoff=0.5, order=4.0, tau=0.1, theta=1.0,
+                        scale=1.0):
+    """Interleaved float coefficients (length 2*nfft) that the ``filter`` task
+    multiplies into the complex spectrum, restated from
+    src/ufo-filter-task.c:162-336.  ``width`` there is the interleaved float
+    width 2*nfft.  Values are computed in double and stored as float, as in the
+    reference; ramp-fromreal's FFT is taken here in FP64."""
+    width = 2 * nfft
+    if width & (width - 1):
+        raise ValueError("Invalid filter input width %u, must be a power of two" % width)
+    f = np.zeros(width, dtype=np.float32)
+    f[0] = f[1] = np.float32(0.5 / width)
+    ftype = FILTERS.index(filter) if isinstance(filter, str) else int(filter)
+    f64 = lambda v: np.float32(v)  # noqa: E731  (double -> gfloat store)
+    scale = float(np.float32(scale))
+    cutoff = float(np.float32(cutoff))
+    order = float(np.float32(order))
+    tau = float(np.float32(tau))
+    theta = float(np.float32(theta))
+    if ftype == 0:  # ramp :171-182
+        step = 2.0 / width
+        for k in range(1, width // 4 + 1):
+            f[2 * k] = f64(k * step * scale)
+            f[2 * k + 1] = f[2 * k]
+    elif ftype == 1:  # ramp-fromreal :184-195
+        f[0] = f[1] = f64(0.25 * scale)
+        for k in range(1, width // 4 + 1):
+            f[2 * k] = f64(-scale / (k * k * math.pi * math.pi)) if k % 2 else 0.0
+            f[2 * k + 1] = f[2 * k]
+    elif ftype == 2:  # butterworth :197-209
+        step = 2.0 / width
+        for k in range(0, width // 4 + 1):
+            fr = k * step
+            f[2 * k] = f64(fr / (1.0 + math.pow(fr / cutoff, 2.0 * order)) * scale)
+            f[2 * k + 1] = f[2 * k]
+    elif ftype == 3:  # faris-byer :254-276
+        pi_squared_tau = math.pi * math.pi * tau
+        sin_theta_2 = -math.sin(theta) / 2
+        padding = _padding_value(width)
+        f[0] = 0
+        for x in range(1, width // 2 + 1):
+            if x % 2 != 0:
+                f[x] = f64(1 / (pi_squared_tau * x))
+        for i in range(width // 2 + 1, width):
+            x = width + 1 - i
+            if x % 2 != 0:
+                f[padding - width - i - 1] = f64(sin_theta_2 / (x * x * pi_squared_tau))
+    elif ftype == 4:  # hamming :211-224
+        step = 2.0 / width
+        for k in range(0, width // 4 + 1):
+            fr = k * step
+            f[2 * k] = f64(fr * (0.54 + 0.46 * math.cos(math.pi * fr / cutoff)) * scale) if fr < cutoff else 0
+            f[2 * k + 1] = f[2 * k]
+    elif ftype == 5:  # bh3 :226-240
+        step = 2.0 / width
+        a0, a1, a2 = 0.42, 0.5, 0.08
+        for k in range(1, width // 4 + 1):
+            fr = k * step
+            f[2 * k] = f64(fr * (a0 + a1 * math.cos(fr * math.pi) + a2 * math.cos(2.0 * fr * math.pi)) * scale)
+            f[2 * k + 1] = f[2 * k]
+    else:
+        raise ValueError("unknown filter %r" % (filter,))
+    _mirror(f, width)
+    out = f.astype(np.float64)
+    if ftype == 1:  # :317-334 forward FFT of the interleaved (h, h) pairs, in place
+        z = np.fft.fft(out[0::2] + 1j * out[1::2])
+        out = np.empty(width, dtype=np.float64)
+        out[0::2] = z.real
+        out[1::2] = z.imag
+    return out
+
+
+def fft_sizes(width, size_x=0, crop_width=0):
+    """(nfft, out_width) of ``fft dimensions=1 [size-x] ! filter ! ifft [crop-width]``:
+    src/ufo-fft-task.c:123-196 (auto-zeropadding is effectively FALSE) and
+    src/ufo-ifft-task.c:111-177 (crop-width defaults to the full FFT width)."""
+    if size_x and size_x < width:
+        raise ValueError("Specified size must be greater than or equal to input size")
+    nfft = size_x if size_x else width
+    if crop_width and crop_width > nfft:
+        raise ValueError("Cropped size must be less than or equal to input size")
+    return nfft, (crop_width if crop_width else nfft)
+
+
+def fft_filter_ifft(sino, size_x=0, crop_width=0, **filter_props):
+    """FP64 ``fft ! filter ! ifft`` over the last axis of ``sino``."""
+    sino = np.asarray(sino, dtype=np.float64)
+    width = sino.shape[-1]
+    nfft, out_w = fft_sizes(width, size_x, crop_width)
+    coeff = filter_coefficients(nfft, **filter_props)
+    X = np.fft.fft(sino, n=nfft, axis=-1)
+    Y = X.real * coeff[0::2] + 1j * (X.imag * coeff[1::2])
+    y = np.fft.ifft(Y, axis=-1).real
+    return y[..., :out_w]
+
+
+# --------------------------------------------------------------------------- backproject
+
+def bp_luts(n_projections, angle_step=0.0, angle_offset=0.0):
+    """src/ufo-backproject-task.c:174-196,245-251: FP64 sin/cos LUTs."""
+    step = angle_step if angle_step > 0.0 else math.pi / n_projections
+    ang = angle_offset + np.arange(n_projections, dtype=np.float64) * step
+    return np.sin(ang), np.cos(ang)
+
+
+def backproject(sino, num_projections=0, offset=0, axis_pos=-1.0, angle_step=-1.0, angle_offset=0.0,
+                mode="texture", roi_x=0, roi_y=0, roi_width=0, roi_height=0, interp=INTERP_EXACT,
+                luts_fp32=False):
+    """``backproject`` of one sinogram [P, W] or a stack [Z, P, W] -> FP64 slices."""
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    squeeze = sino.ndim == 2
+    if squeeze:
+        sino = sino[None]
+    nz, P, W = sino.shape
+    n_proj = num_projections if num_projections else P
+    if P > n_proj:
+        raise ValueError("Total number of projections (%u) must be greater than or equal to "
+                         "sinogram height (%u)" % (n_proj, P))
+    if offset + P > n_proj:
+        raise ValueError("offset + sinogram height exceeds num-projections")
+    rw = roi_width if roi_width else W
+    rh = roi_height if roi_height else W
+    axis = axis_pos if axis_pos > 0.0 else float(np.float32(W) / np.float32(2.0))
+    s, c = bp_luts(n_proj, angle_step if angle_step > 0 else 0.0, angle_offset)
+    if luts_fp32:
+        s = s.astype(np.float32).astype(np.float64)
+        c = c.astype(np.float32).astype(np.float64)
+    if mode == "nearest":
+        interp = INTERP_NEAREST
+    out = np.zeros((nz, rh, rw), dtype=np.float64)
+    lib().oracle_bp_parallel(_p(sino), W, P, nz, _p(s), _p(c), offset, float(np.float32(axis)),
+                             roi_x, roi_y, rw, rh, interp, _p(out))
+    return out[0] if squeeze else out
+
+
+def fbp(sino, axis_pos=-1.0, size_x=0, crop_width=0, filter_props=None, **bp_props):
+    """FP64 ``fft ! filter ! ifft ! backproject``."""
+    filtered = fft_filter_ifft(sino, size_x=size_x, crop_width=crop_width, **(filter_props or {}))
+    return backproject(filtered.astype(np.float32), axis_pos=axis_pos, **bp_props)
+
+
+# --------------------------------------------------------------------------- general backproject
+
+def _almost_zero(values):
+    return all(abs(v) < 1e-7 for v in values)
+
+
+def gbp_flags(geom, parameter="z"):
+    """Geometry-class flags, src/ufo-general-backproject-task.c:1294-1320."""
+    g = {k: list(np.atleast_1d(v)) for k, v in geom.items()}
+    is_axis = parameter in ("axis-angle-x", "axis-angle-y", "axis-angle-z")
+    is_vol = parameter.startswith("volume-angle")
+    is_det_rot = parameter.startswith("detector-angle")
+    is_det_pos = parameter.startswith("detector-position")
+    flags = 0
+    if is_axis or not (_almost_zero(g["axis-angle-x"]) and _almost_zero(g["axis-angle-y"])):
+        flags |= F_WITH_AXIS
+    if is_vol or not (_almost_zero(g["volume-angle-x"]) and _almost_zero(g["volume-angle-y"])
+                      and _almost_zero(g["volume-angle-z"])):
+        flags |= F_WITH_VOLUME
+    if not (_almost_zero(g["detector-position-x"]) and _almost_zero(g["detector-position-z"])):
+        flags |= F_SHIFTED_DETECTOR
+    if not (_almost_zero(g["source-position-x"]) and _almost_zero(g["source-position-z"])):
+        flags |= F_SHIFTED_SOURCE
+    if (not is_det_rot and not is_det_pos and _almost_zero(g["detector-angle-x"])
+            and _almost_zero(g["detector-angle-y"]) and _almost_zero(g["detector-angle-z"])):
+        flags |= F_PERPENDICULAR
+    if all(math.isinf(v) for v in g["source-position-y"]):
+        flags |= F_PARALLEL
+    return flags
+
+
+GBP_DEFAULTS = {
+    "axis-angle-x": 0.0, "axis-angle-y": 0.0,
+    "volume-angle-x": 0.0, "volume-angle-y": 0.0, "volume-angle-z": 0.0,
+    "detector-angle-x": 0.0, "detector-angle-y": 0.0, "detector-angle-z": 0.0,
+    "center-position-x": 0.0, "center-position-z": 0.0,
+    "source-position-x": 0.0, "source-position-y": -math.inf, "source-position-z": 0.0,
+    "detector-position-x": 0.0, "detector-position-y": 0.0, "detector-position-z": 0.0,
+}
+
+
+def gbp_geometry_table(num_projections, overall_angle=2 * math.pi, **geom):
+    """[n_proj, 17] FP64 table; scalars broadcast (ufo-scarray.c:95-108); the
+    tomographic angles default to i / n * overall-angle (:1435-1446)."""
+    n = num_projections
+    table = np.zeros((n, len(GEOM_COLS)), dtype=np.float64)
+    for j, name in enumerate(GEOM_COLS):
+        if name == "axis-angle-z":
+            v = geom.get(name)
+            if v is None or np.size(v) != n:
+                v = np.arange(n, dtype=np.float64) / n * overall_angle
+        else:
+            v = geom.get(name, GBP_DEFAULTS[name])
+            if np.size(v) not in (1, n):
+                raise ValueError("%s must have 1 or num-projections values" % name)
+        table[:, j] = np.broadcast_to(np.asarray(v, dtype=np.float64).reshape(-1), (n,))
+    return table
+
+
+def _region(reg, length):
+    """compute_slice_region (:280-291): (start, step) or (-(length/2), 1)."""
+    if reg is not None and reg[2]:
+        return float(reg[0]), float(reg[2])
+    return -float(np.float32(length) / np.float32(2)), 1.0
+
+
+def _region_size(reg):
+    return int(math.ceil((reg[1] - reg[0]) / reg[2]))
+
+
+def general_backproject(proj, num_projections, region=(0.0, 0.0, 0.0), x_region=(0.0, 0.0, 0.0),
+                        y_region=(0.0, 0.0, 0.0), z=0.0, parameter="z", overall_angle=2 * math.pi,
+                        addressing_mode="clamp", interp=INTERP_EXACT, **geom):
+    """FP64 ``general-backproject`` of projections [n_proj, H, W] -> volume [nz, ny, nx]."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    n, H, W = proj.shape
+    if n != num_projections:
+        raise ValueError("need num-projections projections")
+    nx = W if not x_region[2] else _region_size(x_region)
+    ny = W if not y_region[2] else _region_size(y_region)
+    x0, dx = _region(x_region if x_region[2] else None, nx)
+    y0, dy = _region(y_region if y_region[2] else None, ny)
+    if abs(region[2]) < 1e-7:
+        start, stop, step = 0.0, 1.0, 1.0
+    else:
+        start, stop, step = region
+    nz = int(math.ceil((stop - start) / step))
+    slice_values = start + np.arange(nz, dtype=np.float64) * step
+    table = gbp_geometry_table(n, overall_angle, **geom)
+    flags = gbp_flags({k: geom.get(k, GBP_DEFAULTS.get(k, 0.0)) for k in GEOM_COLS if k != "axis-angle-z"},
+                      parameter)
+    param_col = -1 if parameter == "z" else GEOM_COLS.index(parameter)
+    norm = abs(overall_angle) / n
+    addr = {"clamp": ADDR_CLAMP, "clamp_to_edge": ADDR_CLAMP_TO_EDGE, "none": ADDR_CLAMP_TO_EDGE}[addressing_mode]
+    out = np.zeros((nz, ny, nx), dtype=np.float64)
+    lib().oracle_gbp(_p(proj), W, H, n, _p(table), flags, param_col, _p(slice_values), float(z),
+                     x0, dx, y0, dy, nx, ny, nz, norm, interp, addr, _p(out))
+    return out
+
+
+def forwardproject(slice_img, n_angles, axis_pos, angle_step):
+    img = np.ascontiguousarray(slice_img, dtype=np.float32)
+    W = img.shape[-1]
+    out = np.zeros((n_angles, W), dtype=np.float64)
+    lib().oracle_forwardproject(_p(img), W, n_angles, float(axis_pos), float(angle_step), _p(out))
+    return out
+
+
+# --------------------------------------------------------------------------- phantoms
+
+def random_ellipses(seed, n=10, semi=(0.05, 0.4), density=(-0.5, 1.0)):
+    """Rows (cx, cy, a, b, phi, rho): centres uniform in the unit disc, semi-axes
+    uniform in ``semi``, angles uniform in [0, pi), densities uniform in ``density``."""
+    rng = np.random.default_rng(seed)
+    r = np.sqrt(rng.uniform(0, 1, n))
+    t = rng.uniform(0, 2 * math.pi, n)
+    ell = np.stack([r * np.cos(t), r * np.sin(t), rng.uniform(*semi, n), rng.uniform(*semi, n),
+                    rng.uniform(0, math.pi, n), rng.uniform(*density, n)], axis=1)
+    return np.ascontiguousarray(ell, dtype=np.float64)
+
+
+def ellipse_sinogram(ell, width, angles, axis=None, scale=None):
+    """Analytic parallel-beam sinogram [P, width] in pixel-length units."""
+    axis = width / 2.0 if axis is None else axis
+    scale = width / 2.0 if scale is None else scale
+    angles = np.ascontiguousarray(angles, dtype=np.float64)
+    out = np.zeros((len(angles), width), dtype=np.float64)
+    lib().oracle_ellipse_sinogram(_p(ell), len(ell), width, len(angles), _p(angles), float(axis), float(scale),
+                                  _p(out))
+    return out
+
+
+def ellipse_image(ell, n, axis=None, scale=None, ss=4):
+    axis = n / 2.0 if axis is None else axis
+    scale = n / 2.0 if scale is None else scale
+    out = np.zeros((n, n), dtype=np.float64)
+    lib().oracle_ellipse_image(_p(ell), len(ell), n, float(axis), float(scale), ss, _p(out))
+    return out
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

@@ -1,0 +1,468 @@
+// Parallel-beam backprojection (the `backproject` task).
+//
+// Reference behaviour (src/kernels/backproject.cl:50-94, src/ufo-backproject-task.c:96-267):
+//   bx = x - axis + roi_x + 0.5,  by = y - axis + roi_y + 0.5
+//   h_p = by * sin(theta_p) + bx * cos(theta_p) + axis
+//   slice[y][x] = pi / P * sum_p lerp(sino[p], h_p)
+// with the OpenCL linear sampler: texel i centred at i + 0.5, weights from
+// frac(h - 0.5), and 0 outside the sinogram (CLK_ADDRESS_CLAMP).
+//
+// B200 design.  One CTA owns a TX x TY tile of output pixels for ZT slices of a
+// stack that share the geometry (every slice of a parallel-beam stack uses the
+// same angles), so the coordinate math of a pixel is done once per angle and
+// reused across ZT slices.  For each angle only the detector window that the
+// tile can reach (about sqrt(TX^2 + TY^2) bins) is needed; a producer thread
+// issues one TMA copy (cp.async.bulk.tensor.3d, box = window x 1 angle x ZT
+// slices) per angle into an S-stage shared-memory ring guarded by mbarriers, and
+// TMA's zero fill for out-of-range coordinates reproduces CLK_ADDRESS_CLAMP.
+// Consumers interpolate in software with full FP32 weights (the CPU-OpenCL
+// semantics; GPU texture units quantise the weight to 1/256).  Two storage
+// forms are handled:
+//   SINO_F32         rows of FP32 bins: two 4-byte shared loads per update;
+//   SINO_F16/BF16_PAIRS  32-bit pairs (s[j-1], s[j]) written by the filter
+//                    stage: one 4-byte shared load per update (half the
+//                    shared-memory gather bytes), FP32 accumulation.
+// With `kahan` the sum over each angle block is formed in FP32 and added to the
+// running total with Kahan compensation (cost amortised over the block).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "ufob_internal.h"
+
+namespace ufob {
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of `bar`, giving up after `limit_ns`.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_timer_ns() - t0 > limit_ns) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+static constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
+static constexpr int kErrTmaTimeout = 0x1001;
+
+// ------------------------------------------------------------------ tensor maps
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D map over [nz][P][elems] 4-byte elements; box = (box_x, 1, box_z).
+static ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, uint32_t P, uint32_t nz,
+                                 uint32_t pitch, uint64_t slice_pitch, uint32_t box_x, uint32_t box_z)
+{
+    auto fn = encode_fn();
+    if (!fn) return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[3] = {elems, P, nz};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)slice_pitch * 4};
+    cuuint32_t box[3] = {box_x, 1, box_z};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): elems=%u P=%u nz=%u pitch=%u box=%u,%u",
+                    (int)r, elems, P, nz, pitch, box_x, box_z);
+    return UFOB_OK;
+}
+
+// ------------------------------------------------------------------ sin/cos table
+
+__global__ void k_sincos(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *out)
+{
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    double s, c;
+    sincos(angle_offset + (double)(lut_offset + p) * step, &s, &c);  // FP64, cast to FP32 as the reference LUTs
+    out[p] = make_float2((float)s, (float)c);
+}
+
+ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *d_out,
+                                cudaStream_t stream)
+{
+    if (!P) return UFOB_OK;
+    k_sincos<<<(P + 255) / 256, 256, 0, stream>>>(angle_offset, step, lut_offset, P, d_out);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+// ------------------------------------------------------------------ linear kernel
+
+struct BPArgs {
+    uint32_t P, nz;
+    uint32_t roi_x, roi_y, roi_w, roi_h;
+    float axis, norm;
+    const float2 *sincos;
+    float *out;
+    int *err;
+};
+
+template <int TX, int TY, int ZT, int A, int S>
+struct BPShape {
+    static constexpr int kThreads = 256;
+    static constexpr int kRY = TY / (kThreads / TX);  // output rows per thread
+    static_assert(TX == 32, "one warp spans the tile width");
+    static_assert(kRY >= 1 && kRY * (kThreads / TX) == TY, "tile height");
+    // window of detector elements reachable by the tile, plus interpolation tap,
+    // one guard element on each side and 3 for the 16-byte TMA alignment
+    static constexpr int kSpan = (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
+    static constexpr int kWin = ((kSpan + 2 + 2 + 3) + 3) / 4 * 4;
+    static constexpr int kStageElems = A * ZT * kWin;
+    static constexpr size_t kSmem = (size_t)S * kStageElems * 4 + (size_t)S * A * 4 + (size_t)S * 8 + 128;
+};
+
+template <int KIND>
+__device__ __forceinline__ float2 unpack_pair(uint32_t v)
+{
+    if (KIND == SINO_F16_PAIRS) {
+        __half2 h = *reinterpret_cast<__half2 *>(&v);
+        return __half22float2(h);
+    } else {
+        return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u));
+    }
+}
+
+template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
+__global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUtensorMap map, const BPArgs args)
+{
+    using Sh = BPShape<TX, TY, ZT, A, S>;
+    constexpr int WIN = Sh::kWin;
+    constexpr int RY = Sh::kRY;
+    constexpr int YSTEP = 256 / TX;
+    constexpr bool PAIRS = KIND != SINO_F32;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint32_t *data = reinterpret_cast<uint32_t *>(smem_raw);  // [S][A][ZT][WIN]
+    int *win = reinterpret_cast<int *>(smem_raw + (size_t)S * Sh::kStageElems * 4);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S * Sh::kStageElems * 4 + (size_t)S * A * 4);
+
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * ZT;
+    const uint32_t P = args.P;
+    const int nblk = (int)((P + A - 1) / A);
+    const float axis = args.axis;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    // Producer: stage block `blk` into slot blk % S.
+    auto issue = [&](int blk) {
+        const int slot = blk % S;
+        const int p0 = blk * A;
+        const int nval = min(A, (int)P - p0);
+        mbar_arrive_expect_tx(&full[slot], (uint32_t)(nval * ZT * WIN * 4));
+        const float cx0 = (float)(args.roi_x + x0) - axis + 0.5f, cx1 = cx0 + (float)(TX - 1);
+        const float cy0 = (float)(args.roi_y + y0) - axis + 0.5f, cy1 = cy0 + (float)(TY - 1);
+        for (int a = 0; a < nval; a++) {
+            const float2 sc = args.sincos[p0 + a];
+            float h0 = fmaf(cy0, sc.x, fmaf(cx0, sc.y, axis));
+            float h1 = fmaf(cy0, sc.x, fmaf(cx1, sc.y, axis));
+            float h2 = fmaf(cy1, sc.x, fmaf(cx0, sc.y, axis));
+            float h3 = fmaf(cy1, sc.x, fmaf(cx1, sc.y, axis));
+            float hmin = fminf(fminf(h0, h1), fminf(h2, h3));
+            // first element needed: floor(hmin - 0.5) (+1 for pairs), minus one guard element
+            int e = (int)floorf(hmin - 0.5f) + (PAIRS ? 1 : 0) - 1;
+            e = max(min(e, 1 << 24), -(1 << 24));
+            const int xs = e & ~3;  // 16-byte aligned TMA x coordinate (floor for negatives)
+            win[slot * A + a] = xs;
+            tma_load_3d(data + (size_t)(slot * A + a) * ZT * WIN, &map, &full[slot], xs, p0 + a, z0);
+        }
+    };
+
+    if (tid == 0)
+        for (int b = 0; b < S - 1 && b < nblk; b++) issue(b);
+
+    const int lx = tid % TX, ly = tid / TX;
+    const float bx = (float)(args.roi_x + x0 + lx) - axis + 0.5f;
+    float by[RY];
+#pragma unroll
+    for (int j = 0; j < RY; j++) by[j] = (float)(args.roi_y + y0 + ly + j * YSTEP) - axis + 0.5f;
+
+    float acc[RY][ZT], comp[RY][ZT];
+#pragma unroll
+    for (int j = 0; j < RY; j++)
+#pragma unroll
+        for (int z = 0; z < ZT; z++) acc[j][z] = comp[j][z] = 0.f;
+
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23: adding it rounds to an integer in the mantissa
+    const int kMagicBits = __float_as_int(kMagic);
+    const float eoff = axis - 1.0f + (PAIRS ? 1.0f : 0.0f);  // h - 0.5 - 0.5 (+1 for pairs)
+    bool aborted = false;
+
+    for (int blk = 0; blk < nblk; blk++) {
+        if (tid == 0 && blk + S - 1 < nblk) issue(blk + S - 1);
+        const int slot = blk % S;
+        const uint32_t parity = (uint32_t)((blk / S) & 1);
+        const bool ok = mbar_wait_bounded(&full[slot], parity, kWaitLimitNs);
+        const int p0 = blk * A;
+        const int nval = min(A, (int)P - p0);
+        const uint32_t *sdata = data + (size_t)slot * A * ZT * WIN;
+
+        float part[RY][ZT];
+#pragma unroll
+        for (int j = 0; j < RY; j++)
+#pragma unroll
+            for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
+
+        if (ok) {
+#pragma unroll 2
+            for (int a = 0; a < nval; a++) {
+                const float2 sc = __ldg(&args.sincos[p0 + a]);
+                const int xs = win[slot * A + a];
+                const float t = fmaf(bx, sc.y, eoff - (float)xs);
+                const uint32_t *row = sdata + a * ZT * WIN;
+#pragma unroll
+                for (int j = 0; j < RY; j++) {
+                    const float vv = fmaf(by[j], sc.x, t);  // element coordinate - 0.5
+                    const float r = vv + kMagic;
+                    const float fe = r - kMagic;            // rint(vv) == floor(vv + 0.5)
+                    const float d = vv - fe;
+                    const float w = d + 0.5f, omw = 0.5f - d;
+                    uint32_t e = (uint32_t)(__float_as_int(r) - kMagicBits);
+                    e = min(e, (uint32_t)(WIN - 2));  // guard: never leaves the angle's window
+#pragma unroll
+                    for (int z = 0; z < ZT; z++) {
+                        if (PAIRS) {
+                            const float2 v = unpack_pair<KIND>(row[z * WIN + e]);
+                            part[j][z] = fmaf(omw, v.x, part[j][z]);
+                            part[j][z] = fmaf(w, v.y, part[j][z]);
+                        } else {
+                            const float lo = __uint_as_float(row[z * WIN + e]);
+                            const float hi = __uint_as_float(row[z * WIN + e + 1]);
+                            part[j][z] = fmaf(omw, lo, part[j][z]);
+                            part[j][z] = fmaf(w, hi, part[j][z]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RY; j++)
+#pragma unroll
+            for (int z = 0; z < ZT; z++) {
+                if (KAHAN) {
+                    const float yk = part[j][z] - comp[j][z];
+                    const float tk = acc[j][z] + yk;
+                    comp[j][z] = (tk - acc[j][z]) - yk;
+                    acc[j][z] = tk;
+                } else {
+                    acc[j][z] += part[j][z];
+                }
+            }
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+    }
+
+    if (aborted) {
+        if (tid == 0) {
+            atomicExch(args.err, kErrTmaTimeout);
+            // let every copy that may still be in flight land before the CTA exits
+            for (int s = 0; s < S; s++) {
+                for (int k = 0; k < 2; k++) mbar_wait_bounded(&full[s], (uint32_t)k, kWaitLimitNs / 8);
+            }
+        }
+        return;
+    }
+
+    const float norm = args.norm;
+#pragma unroll
+    for (int j = 0; j < RY; j++) {
+        const int y = y0 + ly + j * YSTEP;
+        const int x = x0 + lx;
+        if (y >= (int)args.roi_h || x >= (int)args.roi_w) continue;
+#pragma unroll
+        for (int z = 0; z < ZT; z++) {
+            if (z0 + z >= (int)args.nz) break;
+            args.out[((size_t)(z0 + z) * args.roi_h + y) * args.roi_w + x] = acc[j][z] * norm;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ nearest kernel
+
+// backproject.cl:24-48: index the flat sinogram with the OUTPUT width as row
+// stride, truncating; indices outside the sinogram read 0 here (the reference
+// has no bounds check).
+__global__ void k_bp_nearest(const float *__restrict__ sino, uint32_t W, uint32_t P, uint32_t pitch,
+                             uint64_t slice_pitch, uint32_t nz, const float2 *__restrict__ sincos, uint32_t roi_x,
+                             uint32_t roi_y, uint32_t roi_w, uint32_t roi_h, float axis, float norm,
+                             float *__restrict__ out)
+{
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    const uint32_t z = blockIdx.z;
+    if (x >= roi_w || y >= roi_h) return;
+    const float bx = (float)x - axis + (float)roi_x + 0.5f;
+    const float by = (float)y - axis + (float)roi_y + 0.5f;
+    const float *s = sino + (size_t)z * slice_pitch;
+    float sum = 0.f;
+    for (uint32_t p = 0; p < P; p++) {
+        const float2 sc = __ldg(&sincos[p]);
+        const float h = axis + bx * sc.y + by * sc.x;
+        const float fi = (float)(p * roi_w) + h;
+        const long long k = (long long)fi;
+        if (k >= 0 && k < (long long)W * P) {
+            // element k of the flat [P][W] sinogram, honouring the caller's pitch
+            const long long row = k / W, col = k % W;
+            sum += __ldg(s + row * pitch + col);
+        }
+    }
+    out[((size_t)z * roi_h + y) * roi_w + x] = sum * norm;
+}
+
+ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t pitch, uint64_t slice_pitch,
+                              float *d_out, cudaStream_t stream)
+{
+    dim3 blk(32, 8), grd((g.roi_w + 31) / 32, (g.roi_h + 7) / 8, g.nz);
+    if (!g.roi_w || !g.roi_h || !g.nz) return UFOB_OK;
+    k_bp_nearest<<<grd, blk, 0, stream>>>(d_sino, g.W, g.P, pitch, slice_pitch, g.nz, g.d_sincos, g.roi_x, g.roi_y,
+                                          g.roi_w, g.roi_h, g.axis, g.norm, d_out);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+// ------------------------------------------------------------------ dispatch
+
+template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
+static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32_t elems, uint32_t pitch,
+                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream)
+{
+    using Sh = BPShape<TX, TY, ZT, A, S>;
+    auto kern = k_bp_linear<TX, TY, ZT, A, S, KIND, KAHAN>;
+    static bool attr = false;
+    if (!attr) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
+        attr = true;
+    }
+    CUtensorMap map;
+    UFOB_TRY(make_sino_map(&map, d_sino, elems, g.P, g.nz, pitch, slice_pitch, Sh::kWin, ZT));
+    BPArgs a;
+    a.P = g.P;
+    a.nz = g.nz;
+    a.roi_x = g.roi_x;
+    a.roi_y = g.roi_y;
+    a.roi_w = g.roi_w;
+    a.roi_h = g.roi_h;
+    a.axis = g.axis;
+    a.norm = g.norm;
+    a.sincos = g.d_sincos;
+    a.out = d_out;
+    a.err = device_error_word();
+    dim3 grid((g.roi_w + TX - 1) / TX, (g.roi_h + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
+    kern<<<grid, Sh::kThreads, Sh::kSmem, stream>>>(map, a);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+template <int KIND, bool KAHAN>
+static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_sino, uint32_t elems, uint32_t pitch,
+                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream)
+{
+    switch (tile) {
+    case 0: return launch_linear<32, 16, 1, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 1: return launch_linear<32, 32, 2, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 2: return launch_linear<32, 32, 4, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 3: return launch_linear<32, 16, 4, 16, 4, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 4: return launch_linear<32, 32, 8, 8, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    default: return fail(UFOB_ERR_INVALID, "backproject: unknown tile id %d", tile);
+    }
+}
+
+static int default_tile(const BPGeometry &g)
+{
+    if (g.nz == 1) return 0;
+    if (g.nz == 2) return 1;
+    return 2;
+}
+
+ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
+                             uint64_t slice_pitch, float *d_out, bool kahan, int tile, cudaStream_t stream)
+{
+    if (!g.roi_w || !g.roi_h || !g.nz || !g.P) return UFOB_OK;
+    if (((uintptr_t)d_sino & 15) || (pitch & 3) || (slice_pitch & 3))
+        return fail(UFOB_ERR_INVALID, "backproject: sinogram base/pitches must be 16-byte aligned");
+    if (tile < 0) tile = default_tile(g);
+    const uint32_t elems = kind == SINO_F32 ? g.W : g.W + 1;  // pairs: (s[j-1], s[j]) for j = 0..W
+    if (kind == SINO_F32) {
+        return kahan ? dispatch_tile<SINO_F32, true>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream)
+                     : dispatch_tile<SINO_F32, false>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    } else if (kind == SINO_F16_PAIRS) {
+        return kahan ? dispatch_tile<SINO_F16_PAIRS, true>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream)
+                     : dispatch_tile<SINO_F16_PAIRS, false>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    } else {
+        return kahan ? dispatch_tile<SINO_BF16_PAIRS, true>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream)
+                     : dispatch_tile<SINO_BF16_PAIRS, false>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    }
+}
+
+}  // namespace ufob

@@ -1,0 +1,645 @@
+// C ABI: task objects mirroring the reference's `filter` (with its fft/ifft
+// neighbours), `backproject` and the fused FBP chain.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+#include <strings.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "ufob_internal.h"
+
+namespace ufob {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+ufob_status fail(ufob_status st, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+ufob_status cuda_fail(cudaError_t e, const char *what)
+{
+    cudaGetLastError();  // clear a sticky launch error so the caller can retry with other sizes
+    return fail(e == cudaErrorMemoryAllocation ? UFOB_ERR_NOMEM : UFOB_ERR_CUDA, "%s: %s (%s)", what,
+                cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+ufob_status DevBuf::ensure(size_t n)
+{
+    if (n <= bytes && ptr) return UFOB_OK;
+    release();
+    if (!n) return UFOB_OK;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return cuda_fail(e, "cudaMalloc");
+    }
+    bytes = n;
+    return UFOB_OK;
+}
+
+static int g_num_sms = 0;
+
+ufob_status ensure_device()
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice (no usable CUDA device)");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return fail(UFOB_ERR_CUDA, "device %d (%s) is sm_%d%d; this engine is built for sm_100a only", dev, prop.name,
+                    prop.major, prop.minor);
+    g_num_sms = prop.multiProcessorCount;
+    return UFOB_OK;
+}
+
+int num_sms()
+{
+    if (!g_num_sms) ensure_device();
+    return g_num_sms ? g_num_sms : 148;
+}
+
+__device__ int g_device_error = 0;
+
+int *device_error_word()
+{
+    void *p = nullptr;
+    cudaGetSymbolAddress(&p, g_device_error);
+    return reinterpret_cast<int *>(p);
+}
+
+ufob_status check_device_error_word(cudaStream_t stream)
+{
+    int v = 0, zero = 0;
+    UFOB_CUDA_TRY(cudaMemcpyFromSymbolAsync(&v, g_device_error, sizeof v, 0, cudaMemcpyDeviceToHost, stream));
+    UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (v) {
+        UFOB_CUDA_TRY(cudaMemcpyToSymbol(g_device_error, &zero, sizeof zero));
+        return fail(UFOB_ERR_TIMEOUT, "a device-side bounded wait gave up (code 0x%x)", v);
+    }
+    return UFOB_OK;
+}
+
+static bool streq(const char *a, const char *b) { return a && b && strcasecmp(a, b) == 0; }
+
+// property names may use '-' or '_' (GObject canonicalises both)
+static bool prop_is(const char *name, const char *canon)
+{
+    if (!name) return false;
+    for (; *name && *canon; name++, canon++) {
+        char a = *name == '_' ? '-' : *name;
+        if (a != *canon) return false;
+    }
+    return *name == 0 && *canon == 0;
+}
+
+}  // namespace ufob
+
+using namespace ufob;
+
+// =================================================================== filter
+
+struct ufob_filter {
+    ufob_filter_props props;
+    FilterPlan plan;
+};
+
+static const char *kFilterNames[] = {"ramp", "ramp-fromreal", "butterworth", "faris-byer", "hamming", "bh3"};
+
+extern "C" {
+
+const char *ufob_last_error(void) { return g_last_error.c_str(); }
+
+const char *ufob_status_string(ufob_status s)
+{
+    switch (s) {
+    case UFOB_OK: return "ok";
+    case UFOB_ERR_INVALID: return "invalid argument";
+    case UFOB_ERR_SETUP: return "setup error";
+    case UFOB_ERR_REQUISITION: return "get_requisition error";
+    case UFOB_ERR_CUDA: return "CUDA error";
+    case UFOB_ERR_NOMEM: return "out of device memory";
+    case UFOB_ERR_TIMEOUT: return "device wait timed out";
+    case UFOB_ERR_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown status";
+}
+
+ufob_status ufob_device_check(int *cc_major, int *cc_minor, int *nsm)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    if (cc_major) *cc_major = prop.major;
+    if (cc_minor) *cc_minor = prop.minor;
+    if (nsm) *nsm = prop.multiProcessorCount;
+    return ensure_device();
+}
+
+void ufob_filter_props_init(ufob_filter_props *p)
+{
+    // src/ufo-filter-task.c:531-545, src/ufo-fft-task.c:541-568, src/ufo-ifft-task.c:496-515
+    p->filter = UFOB_FILTER_RAMP_FROMREAL;
+    p->cutoff = 0.5f;
+    p->order = 4.0f;
+    p->tau = 0.1f;
+    p->theta = 1.0f;
+    p->scale = 1.0f;
+    p->size_x = 0;
+    p->crop_width = 0;
+}
+
+static ufob_status validate_filter_props(const ufob_filter_props *p)
+{
+    if (p->filter < 0 || p->filter > UFOB_FILTER_BH3) return fail(UFOB_ERR_INVALID, "filter: unknown filter %d", p->filter);
+    if (!(p->cutoff >= 0.f && p->cutoff <= 1.f)) return fail(UFOB_ERR_INVALID, "filter: cutoff %g outside [0, 1]", p->cutoff);
+    if (!(p->order >= 2.f && p->order <= 32.f)) return fail(UFOB_ERR_INVALID, "filter: order %g outside [2, 32]", p->order);
+    if (p->size_x > 32768) return fail(UFOB_ERR_INVALID, "fft: size-x %u outside [0, 32768]", p->size_x);
+    if (p->crop_width > 32768) return fail(UFOB_ERR_INVALID, "ifft: crop-width %u outside [0, 32768]", p->crop_width);
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_create(const ufob_filter_props *props, ufob_filter **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "filter_create: out is NULL");
+    ufob_filter_props p;
+    ufob_filter_props_init(&p);
+    if (props) p = *props;
+    UFOB_TRY(validate_filter_props(&p));
+    ufob_filter *f = new ufob_filter;
+    f->props = p;
+    *out = f;
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_set_property(ufob_filter *f, const char *name, double v)
+{
+    if (!f) return fail(UFOB_ERR_INVALID, "filter handle is NULL");
+    ufob_filter_props p = f->props;
+    if (prop_is(name, "filter")) p.filter = (int)v;
+    else if (prop_is(name, "cutoff")) p.cutoff = (float)v;
+    else if (prop_is(name, "order")) p.order = (float)v;
+    else if (prop_is(name, "tau")) p.tau = (float)v;
+    else if (prop_is(name, "theta")) p.theta = (float)v;
+    else if (prop_is(name, "scale")) p.scale = (float)v;
+    else if (prop_is(name, "size-x")) { if (v < 0 || v > 32768) return fail(UFOB_ERR_INVALID, "size-x out of range"); p.size_x = (uint32_t)v; }
+    else if (prop_is(name, "crop-width")) { if (v < 0 || v > 32768) return fail(UFOB_ERR_INVALID, "crop-width out of range"); p.crop_width = (uint32_t)v; }
+    else return fail(UFOB_ERR_INVALID, "filter: no property named '%s'", name ? name : "(null)");
+    UFOB_TRY(validate_filter_props(&p));
+    f->props = p;
+    f->plan.nfft = 0;  // coefficients depend on every property
+    f->plan.coeff.clear();
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_set_property_string(ufob_filter *f, const char *name, const char *value)
+{
+    if (!f) return fail(UFOB_ERR_INVALID, "filter handle is NULL");
+    if (prop_is(name, "filter")) {
+        for (int i = 0; i < 6; i++)
+            if (streq(value, kFilterNames[i])) return ufob_filter_set_property(f, name, i);
+        return fail(UFOB_ERR_INVALID, "filter: unknown filter '%s'", value ? value : "(null)");
+    }
+    char *end = nullptr;
+    double v = value ? strtod(value, &end) : 0.0;
+    if (!value || end == value) return fail(UFOB_ERR_INVALID, "filter: '%s' is not a number", value ? value : "(null)");
+    return ufob_filter_set_property(f, name, v);
+}
+
+static ufob_status filter_sizes(const ufob_filter_props &p, uint32_t width, uint32_t *nfft, uint32_t *out_w)
+{
+    if (!width) return fail(UFOB_ERR_REQUISITION, "fft: input width is 0");
+    if (p.size_x && p.size_x < width)
+        return fail(UFOB_ERR_REQUISITION, "Specified size must be greater than or equal to input size");
+    uint32_t n = p.size_x ? p.size_x : width;
+    if (!is_pow2(2ull * n))
+        return fail(UFOB_ERR_REQUISITION, "Invalid filter input width %u, must be a power of two", 2 * n);
+    if (p.crop_width > n) return fail(UFOB_ERR_REQUISITION, "Cropped size must be less than or equal to input size");
+    *nfft = n;
+    *out_w = p.crop_width ? p.crop_width : n;
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_get_requisition(ufob_filter *f, uint32_t width, uint32_t height, uint32_t *ow, uint32_t *oh)
+{
+    if (!f) return fail(UFOB_ERR_INVALID, "filter handle is NULL");
+    uint32_t n, w;
+    UFOB_TRY(filter_sizes(f->props, width, &n, &w));
+    if (ow) *ow = w;
+    if (oh) *oh = height;
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_run(ufob_filter *f, const float *d_in, uint32_t width, uint32_t rows, uint32_t in_pitch,
+                            void *d_out, ufob_dtype out_dtype, ufob_layout out_layout, uint32_t out_pitch,
+                            void *stream)
+{
+    if (!f || !d_in || !d_out) return fail(UFOB_ERR_INVALID, "filter_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t n, w;
+    UFOB_TRY(filter_sizes(f->props, width, &n, &w));
+    cudaStream_t s = (cudaStream_t)stream;
+    UFOB_TRY(filter_plan_build(f->props, n, f->plan, s));
+    if (!in_pitch) in_pitch = width;
+    if (!out_pitch) out_pitch = out_layout == UFOB_LAYOUT_PAIRS ? round_up(w + 1, 4) : w;
+    return filter_rows_launch(f->plan, d_in, width, rows, in_pitch, d_out, out_dtype, out_layout, w, out_pitch, s);
+}
+
+ufob_status ufob_filter_coefficients(ufob_filter *f, uint32_t width, float *host_out, uint32_t count)
+{
+    if (!f || !host_out) return fail(UFOB_ERR_INVALID, "filter_coefficients: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t n, w;
+    UFOB_TRY(filter_sizes(f->props, width, &n, &w));
+    UFOB_TRY(filter_plan_build(f->props, n, f->plan, 0));
+    if (count < 2 * n) return fail(UFOB_ERR_INVALID, "filter_coefficients: need room for %u floats", 2 * n);
+    memcpy(host_out, f->plan.coeff.data(), sizeof(float) * 2 * n);
+    return UFOB_OK;
+}
+
+ufob_status ufob_filter_apply_spectrum(ufob_filter *f, const float *d_in, float *d_out, uint32_t width2,
+                                       uint32_t rows, void *stream)
+{
+    if (!f || !d_in || !d_out) return fail(UFOB_ERR_INVALID, "filter_apply_spectrum: NULL argument");
+    UFOB_TRY(ensure_device());
+    if (!is_pow2(width2))
+        return fail(UFOB_ERR_REQUISITION, "Invalid filter input width %u, must be a power of two", width2);
+    UFOB_TRY(filter_plan_build(f->props, width2 / 2, f->plan, (cudaStream_t)stream));
+    return filter_spectrum_launch(f->plan.d_coeff.as<float>(), d_in, d_out, width2, rows, (cudaStream_t)stream);
+}
+
+void ufob_filter_destroy(ufob_filter *f) { delete f; }
+
+}  // extern "C"
+
+// =================================================================== backproject
+
+struct ufob_backproject {
+    ufob_bp_props props;
+    DevBuf sincos;
+    DevBuf aligned;  // copy of a sinogram whose pitch is not TMA-compatible
+    // cache key of the sin/cos table
+    uint32_t key_P = 0, key_nproj = 0, key_offset = 0;
+    double key_step = 0, key_aoff = 0;
+};
+
+extern "C" {
+
+void ufob_bp_props_init(ufob_bp_props *p)
+{
+    // src/ufo-backproject-task.c:520-541
+    p->num_projections = 0;
+    p->offset = 0;
+    p->axis_pos = -1.0;
+    p->angle_step = -1.0;
+    p->angle_offset = 0.0;
+    p->mode = UFOB_BP_TEXTURE;
+    p->roi_x = p->roi_y = 0;
+    p->roi_width = p->roi_height = 0;
+    p->compensated = -1;
+    p->tile = -1;
+}
+
+static ufob_status validate_bp_props(const ufob_bp_props *p)
+{
+    if (p->num_projections > 32768) return fail(UFOB_ERR_INVALID, "num-projections outside [0, 32768]");
+    if (p->offset > 32768) return fail(UFOB_ERR_INVALID, "offset outside [0, 32768]");
+    if (!(p->axis_pos >= -1.0 && p->axis_pos <= 32768.0)) return fail(UFOB_ERR_INVALID, "axis-pos outside [-1, 32768]");
+    if (!(p->angle_offset >= 0.0)) return fail(UFOB_ERR_INVALID, "angle-offset must be >= 0");
+    if (p->mode != UFOB_BP_NEAREST && p->mode != UFOB_BP_TEXTURE) return fail(UFOB_ERR_INVALID, "unknown mode %d", p->mode);
+    return UFOB_OK;
+}
+
+ufob_status ufob_backproject_create(const ufob_bp_props *props, ufob_backproject **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "backproject_create: out is NULL");
+    ufob_bp_props p;
+    ufob_bp_props_init(&p);
+    if (props) p = *props;
+    UFOB_TRY(validate_bp_props(&p));
+    ufob_backproject *bp = new ufob_backproject;
+    bp->props = p;
+    *out = bp;
+    return UFOB_OK;
+}
+
+ufob_status ufob_backproject_set_property(ufob_backproject *bp, const char *name, double v)
+{
+    if (!bp) return fail(UFOB_ERR_INVALID, "backproject handle is NULL");
+    ufob_bp_props p = bp->props;
+    if (prop_is(name, "num-projections")) p.num_projections = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "offset")) p.offset = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "axis-pos")) p.axis_pos = v;
+    else if (prop_is(name, "angle-step")) p.angle_step = v;
+    else if (prop_is(name, "angle-offset")) p.angle_offset = v;
+    else if (prop_is(name, "mode")) p.mode = (int)v;
+    else if (prop_is(name, "roi-x")) p.roi_x = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "roi-y")) p.roi_y = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "roi-width")) p.roi_width = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "roi-height")) p.roi_height = (uint32_t)std::max(0.0, v);
+    else if (prop_is(name, "compensated")) p.compensated = (int)v;
+    else if (prop_is(name, "tile")) p.tile = (int)v;
+    else return fail(UFOB_ERR_INVALID, "backproject: no property named '%s'", name ? name : "(null)");
+    if ((prop_is(name, "num-projections") || prop_is(name, "offset") || prop_is(name, "roi-x") ||
+         prop_is(name, "roi-y") || prop_is(name, "roi-width") || prop_is(name, "roi-height")) && v < 0)
+        return fail(UFOB_ERR_INVALID, "backproject: '%s' must be >= 0", name);
+    UFOB_TRY(validate_bp_props(&p));
+    bp->props = p;
+    return UFOB_OK;
+}
+
+ufob_status ufob_backproject_set_property_string(ufob_backproject *bp, const char *name, const char *value)
+{
+    if (!bp) return fail(UFOB_ERR_INVALID, "backproject handle is NULL");
+    if (prop_is(name, "mode")) {
+        if (streq(value, "nearest")) return ufob_backproject_set_property(bp, name, UFOB_BP_NEAREST);
+        if (streq(value, "texture")) return ufob_backproject_set_property(bp, name, UFOB_BP_TEXTURE);
+        return fail(UFOB_ERR_INVALID, "backproject: unknown mode '%s'", value ? value : "(null)");
+    }
+    char *end = nullptr;
+    double v = value ? strtod(value, &end) : 0.0;
+    if (!value || end == value) return fail(UFOB_ERR_INVALID, "backproject: '%s' is not a number", value ? value : "(null)");
+    return ufob_backproject_set_property(bp, name, v);
+}
+
+static ufob_status bp_sizes(const ufob_bp_props &p, uint32_t width, uint32_t height, uint32_t *nproj, uint32_t *ow,
+                            uint32_t *oh)
+{
+    if (!width || !height) return fail(UFOB_ERR_REQUISITION, "backproject: empty sinogram %ux%u", width, height);
+    uint32_t n = p.num_projections ? p.num_projections : height;
+    if (height > n)
+        return fail(UFOB_ERR_REQUISITION,
+                    "Total number of projections (%u) must be greater than or equal to sinogram height (%u)", n, height);
+    if ((uint64_t)p.offset + height > n)
+        return fail(UFOB_ERR_REQUISITION, "offset (%u) + sinogram height (%u) exceeds the %u angle table entries",
+                    p.offset, height, n);
+    *nproj = n;
+    *ow = p.roi_width ? p.roi_width : width;
+    *oh = p.roi_height ? p.roi_height : width;  // src/ufo-backproject-task.c:239-244
+    return UFOB_OK;
+}
+
+ufob_status ufob_backproject_get_requisition(ufob_backproject *bp, uint32_t width, uint32_t height, uint32_t *ow,
+                                             uint32_t *oh)
+{
+    if (!bp) return fail(UFOB_ERR_INVALID, "backproject handle is NULL");
+    uint32_t n, w, h;
+    UFOB_TRY(bp_sizes(bp->props, width, height, &n, &w, &h));
+    if (ow) *ow = w;
+    if (oh) *oh = h;
+    return UFOB_OK;
+}
+
+}  // extern "C"
+
+// Prepare the geometry (sin/cos table on the device) for one run.
+static ufob_status bp_prepare(ufob_backproject *bp, uint32_t width, uint32_t height, uint32_t nslices, BPGeometry &g,
+                              cudaStream_t s)
+{
+    uint32_t nproj, ow, oh;
+    UFOB_TRY(bp_sizes(bp->props, width, height, &nproj, &ow, &oh));
+    const ufob_bp_props &p = bp->props;
+    const double step = p.angle_step > 0.0 ? p.angle_step : M_PI / (double)nproj;
+    if (bp->key_P != height || bp->key_nproj != nproj || bp->key_offset != p.offset || bp->key_step != step ||
+        bp->key_aoff != p.angle_offset || !bp->sincos.ptr) {
+        UFOB_TRY(bp->sincos.ensure(sizeof(float2) * height));
+        UFOB_TRY(sincos_table_launch(p.angle_offset, step, p.offset, height, bp->sincos.as<float2>(), s));
+        bp->key_P = height;
+        bp->key_nproj = nproj;
+        bp->key_offset = p.offset;
+        bp->key_step = step;
+        bp->key_aoff = p.angle_offset;
+    }
+    g.W = width;
+    g.P = height;
+    g.nz = nslices;
+    g.roi_x = p.roi_x;
+    g.roi_y = p.roi_y;
+    g.roi_w = ow;
+    g.roi_h = oh;
+    // axis-pos <= 0: width / 2 in float (src/ufo-backproject-task.c:125-134)
+    g.axis = p.axis_pos <= 0.0 ? (float)width / 2.0f : (float)p.axis_pos;
+    g.norm = (float)M_PI / (float)height;  // M_PI_F / n_projections with n = sinogram height (backproject.cl:93)
+    g.d_sincos = bp->sincos.as<float2>();
+    return UFOB_OK;
+}
+
+static bool want_kahan(const ufob_bp_props &p, SinoKind kind, uint32_t P)
+{
+    if (p.compensated >= 0) return p.compensated != 0;
+    return kind != SINO_F32 && P >= 1500;
+}
+
+extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_dtype dtype,
+                                            ufob_layout layout, uint32_t width, uint32_t height, uint32_t nslices,
+                                            uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream)
+{
+    if (!bp || !d_sino || !d_out) return fail(UFOB_ERR_INVALID, "backproject_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    cudaStream_t s = (cudaStream_t)stream;
+    BPGeometry g;
+    UFOB_TRY(bp_prepare(bp, width, height, nslices, g, s));
+    SinoKind kind;
+    if (dtype == UFOB_F32 && layout == UFOB_LAYOUT_ROWS) kind = SINO_F32;
+    else if (dtype == UFOB_F16 && layout == UFOB_LAYOUT_PAIRS) kind = SINO_F16_PAIRS;
+    else if (dtype == UFOB_BF16 && layout == UFOB_LAYOUT_PAIRS) kind = SINO_BF16_PAIRS;
+    else return fail(UFOB_ERR_INVALID, "backproject: sinogram must be F32 rows or F16/BF16 pairs");
+    const uint32_t elems = kind == SINO_F32 ? width : width + 1;
+    if (!pitch) pitch = kind == SINO_F32 ? width : round_up(width + 1, 4);
+    if (pitch < elems) return fail(UFOB_ERR_INVALID, "backproject: pitch %u < row length %u", pitch, elems);
+    if (!slice_pitch) slice_pitch = (uint64_t)pitch * height;
+    if (bp->props.mode == UFOB_BP_NEAREST) {
+        if (kind != SINO_F32) return fail(UFOB_ERR_INVALID, "backproject: mode=nearest needs an F32 sinogram");
+        return bp_nearest_launch(g, (const float *)d_sino, pitch, slice_pitch, d_out, s);
+    }
+    const void *src = d_sino;
+    if (((uintptr_t)d_sino & 15) || (pitch & 3) || (slice_pitch & 3)) {
+        // TMA needs 16-byte aligned rows: restage into an aligned copy
+        const uint32_t ap = round_up(elems, 4);
+        UFOB_TRY(bp->aligned.ensure((size_t)ap * 4 * height * nslices));
+        for (uint32_t z = 0; z < nslices; z++)
+            UFOB_CUDA_TRY(cudaMemcpy2DAsync(bp->aligned.as<char>() + (size_t)z * ap * 4 * height, (size_t)ap * 4,
+                                            (const char *)d_sino + (size_t)z * slice_pitch * 4, (size_t)pitch * 4,
+                                            (size_t)elems * 4, height, cudaMemcpyDeviceToDevice, s));
+        src = bp->aligned.ptr;
+        pitch = ap;
+        slice_pitch = (uint64_t)ap * height;
+    }
+    return bp_linear_launch(g, src, kind, pitch, slice_pitch, d_out, want_kahan(bp->props, kind, height),
+                            bp->props.tile, s);
+}
+
+extern "C" void ufob_backproject_destroy(ufob_backproject *bp) { delete bp; }
+
+// =================================================================== fused FBP
+
+struct ufob_fbp {
+    ufob_filter *f = nullptr;
+    ufob_backproject *bp = nullptr;
+    ufob_dtype storage = UFOB_F32;
+    DevBuf work;        // filtered sinograms of one slice group
+    DevBuf hin[2];      // device staging of host input chunks
+    DevBuf hout[2];     // device staging of host output chunks
+    cudaStream_t s_copy = nullptr, s_comp = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    ~ufob_fbp()
+    {
+        ufob_filter_destroy(f);
+        ufob_backproject_destroy(bp);
+        for (int i = 0; i < 2; i++) {
+            if (ev_in[i]) cudaEventDestroy(ev_in[i]);
+            if (ev_done[i]) cudaEventDestroy(ev_done[i]);
+            if (ev_out[i]) cudaEventDestroy(ev_out[i]);
+        }
+        if (s_copy) cudaStreamDestroy(s_copy);
+        if (s_comp) cudaStreamDestroy(s_comp);
+    }
+};
+
+extern "C" ufob_status ufob_fbp_create(const ufob_filter_props *fp, const ufob_bp_props *bpp, ufob_dtype storage,
+                                       ufob_fbp **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "fbp_create: out is NULL");
+    if (storage != UFOB_F32 && storage != UFOB_F16 && storage != UFOB_BF16)
+        return fail(UFOB_ERR_INVALID, "fbp: storage must be F32, F16 or BF16");
+    ufob_fbp *x = new ufob_fbp;
+    ufob_status st = ufob_filter_create(fp, &x->f);
+    if (st == UFOB_OK) st = ufob_backproject_create(bpp, &x->bp);
+    if (st != UFOB_OK) {
+        delete x;
+        return st;
+    }
+    x->storage = storage;
+    *out = x;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_fbp_get_requisition(ufob_fbp *x, uint32_t width, uint32_t height, uint32_t *ow,
+                                                uint32_t *oh)
+{
+    if (!x) return fail(UFOB_ERR_INVALID, "fbp handle is NULL");
+    uint32_t fw, fh;
+    UFOB_TRY(ufob_filter_get_requisition(x->f, width, height, &fw, &fh));
+    return ufob_backproject_get_requisition(x->bp, fw, fh, ow, oh);
+}
+
+// Filter + backproject `nz` slices already on the device.
+static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, uint32_t height, uint32_t nz,
+                             float *d_out, cudaStream_t s)
+{
+    uint32_t nfft, fw;
+    UFOB_TRY(filter_sizes(x->f->props, width, &nfft, &fw));
+    UFOB_TRY(filter_plan_build(x->f->props, nfft, x->f->plan, s));
+    const bool pairs = x->storage != UFOB_F32;
+    const uint32_t pitch = pairs ? round_up(fw + 1, 4) : round_up(fw, 4);
+    UFOB_TRY(x->work.ensure((size_t)pitch * 4 * height * nz));
+    UFOB_TRY(filter_rows_launch(x->f->plan, d_sino, width, height * nz, width, x->work.ptr, x->storage,
+                                pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw, pitch, s));
+    return ufob_backproject_run(x->bp, x->work.ptr, x->storage, pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw, height,
+                                nz, pitch, (uint64_t)pitch * height, d_out, s);
+}
+
+static uint32_t group_slices(uint32_t width, uint32_t height, uint32_t nslices)
+{
+    // bound the filtered workspace to ~2 GiB, in multiples of 8 slices
+    const uint64_t per_slice = (uint64_t)(width + 4) * 4 * height;
+    uint64_t g = std::max<uint64_t>(8, (2ull << 30) / std::max<uint64_t>(per_slice, 1));
+    g = g / 8 * 8;
+    return (uint32_t)std::min<uint64_t>(g, nslices);
+}
+
+extern "C" ufob_status ufob_fbp_run(ufob_fbp *x, const float *d_sino, uint32_t width, uint32_t height,
+                                    uint32_t nslices, float *d_out, void *stream)
+{
+    if (!x || !d_sino || !d_out) return fail(UFOB_ERR_INVALID, "fbp_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t ow, oh;
+    UFOB_TRY(ufob_fbp_get_requisition(x, width, height, &ow, &oh));
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t G = group_slices(width, height, nslices);
+    for (uint32_t z = 0; z < nslices; z += G) {
+        const uint32_t nz = std::min(G, nslices - z);
+        UFOB_TRY(fbp_group(x, d_sino + (size_t)z * width * height, width, height, nz, d_out + (size_t)z * ow * oh, s));
+    }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint32_t width, uint32_t height,
+                                         uint32_t nslices, float *h_out, uint32_t chunk)
+{
+    if (!x || !h_sino || !h_out) return fail(UFOB_ERR_INVALID, "fbp_run_host: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t ow, oh;
+    UFOB_TRY(ufob_fbp_get_requisition(x, width, height, &ow, &oh));
+    if (!chunk) chunk = 32;
+    chunk = std::min(chunk, nslices);
+    if (!x->s_copy) {
+        UFOB_CUDA_TRY(cudaStreamCreateWithFlags(&x->s_copy, cudaStreamNonBlocking));
+        UFOB_CUDA_TRY(cudaStreamCreateWithFlags(&x->s_comp, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) {
+            UFOB_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_in[i], cudaEventDisableTiming));
+            UFOB_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_done[i], cudaEventDisableTiming));
+            UFOB_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_out[i], cudaEventDisableTiming));
+        }
+    }
+    const size_t in_bytes = (size_t)chunk * width * height * 4, out_bytes = (size_t)chunk * ow * oh * 4;
+    for (int i = 0; i < 2; i++) {
+        UFOB_TRY(x->hin[i].ensure(in_bytes));
+        UFOB_TRY(x->hout[i].ensure(out_bytes));
+    }
+    // Pipeline: H2D(c) on the copy stream -> filter+BP(c) on the compute stream -> D2H(c) on the copy stream,
+    // double-buffered so chunk c+1's upload and chunk c-1's download overlap chunk c's compute.
+    uint32_t c = 0;
+    for (uint32_t z = 0; z < nslices; z += chunk, c++) {
+        const int b = c & 1;
+        const uint32_t nz = std::min(chunk, nslices - z);
+        if (c >= 2) UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_copy, x->ev_done[b], 0));  // hin[b] free again
+        UFOB_CUDA_TRY(cudaMemcpyAsync(x->hin[b].ptr, h_sino + (size_t)z * width * height, (size_t)nz * width * height * 4,
+                                      cudaMemcpyHostToDevice, x->s_copy));
+        UFOB_CUDA_TRY(cudaEventRecord(x->ev_in[b], x->s_copy));
+        UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_comp, x->ev_in[b], 0));
+        if (c >= 2) UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_comp, x->ev_out[b], 0));  // hout[b] downloaded
+        UFOB_TRY(fbp_group(x, x->hin[b].as<float>(), width, height, nz, x->hout[b].as<float>(), x->s_comp));
+        UFOB_CUDA_TRY(cudaEventRecord(x->ev_done[b], x->s_comp));
+        UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_copy, x->ev_done[b], 0));
+        UFOB_CUDA_TRY(cudaMemcpyAsync(h_out + (size_t)z * ow * oh, x->hout[b].ptr, (size_t)nz * ow * oh * 4,
+                                      cudaMemcpyDeviceToHost, x->s_copy));
+        UFOB_CUDA_TRY(cudaEventRecord(x->ev_out[b], x->s_copy));
+    }
+    UFOB_CUDA_TRY(cudaStreamSynchronize(x->s_copy));
+    UFOB_CUDA_TRY(cudaStreamSynchronize(x->s_comp));
+    return check_device_error_word(x->s_comp);
+}
+
+extern "C" void ufob_fbp_destroy(ufob_fbp *x) { delete x; }
+
+extern "C" ufob_status ufob_device_status(void)
+{
+    UFOB_TRY(ensure_device());
+    return check_device_error_word(0);
+}

@@ -1,0 +1,420 @@
+// Ramp-filter stage: the reference's `fft ! filter ! ifft` chain fused into one
+// kernel per pair of sinogram rows.
+//
+// Reference behaviour restated here:
+//  * src/ufo-fft-task.c:123-196,293-304 and src/kernels/fft.cl:20-48 -- each
+//    row of width W is zero-padded to the FFT width N (fft "size-x", default W)
+//    and transformed forward (e^{-2 pi i ...}).
+//  * src/ufo-filter-task.c:162-336 -- a vector of 2N interleaved float
+//    coefficients c is built once; src/kernels/filter.cl:20-29 multiplies the
+//    real part of bin k by c[2k] and the imaginary part by c[2k+1].
+//  * src/ufo-ifft-task.c:287-311 and src/kernels/fft.cl:50-82 -- backward FFT,
+//    real part, crop to "crop-width", scale by 1/N.
+//
+// B200 formulation.  The real part of the inverse transform only depends on
+// the Hermitian part of the filtered spectrum, so for a real row with spectrum
+// X the result equals C2R(G . X) with per-bin gains
+//   G[k] = ((c[2k] + c[2(N-k)]) / 2, (c[2k+1] + c[2(N-k)+1]) / 2),  k = 0..N/2,
+// applied to the real and imaginary parts separately.  This is exact for every
+// coefficient vector the reference can build (also the non-symmetric
+// faris-byer one).  Two real rows a, b are transformed as one complex signal
+// z = a + i b; their spectra are separated, filtered and recombined in shared
+// memory, so one complex FFT pair serves two rows.  The FFT is a radix-4 (plus
+// one radix-2 pass for odd log2 N) Stockham transform in shared memory, with
+// twiddles computed in FP64 and staged into shared memory once per CTA.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include <algorithm>
+
+#include "ufob_internal.h"
+
+namespace ufob {
+
+static constexpr uint32_t kMaxFusedFFT = 8192;
+static constexpr int kFilterThreads = 256;
+
+// ------------------------------------------------------------ host coefficient code
+
+static uint32_t padding_value(uint32_t x)  // src/ufo-filter-task.c:242-252
+{
+    uint32_t padding = 2 * x, result = 1;
+    while (result < padding) result *= 2;
+    return result;
+}
+
+bool build_filter_coefficients(const ufob_filter_props &p, uint32_t nfft, std::vector<float> &f)
+{
+    const uint32_t width = 2 * nfft;  // interleaved float width, as the reference's requisition
+    if (!is_pow2(width)) {
+        set_error("Invalid filter input width %u, must be a power of two", width);
+        return false;
+    }
+    f.assign(width, 0.f);
+    f[0] = f[1] = (float)(0.5 / width);
+    const double scale = p.scale, cutoff = p.cutoff, order = p.order, tau = p.tau, theta = p.theta;
+    const double step = 2.0 / width;
+    switch (p.filter) {
+    case UFOB_FILTER_RAMP:
+        for (uint32_t k = 1; k < width / 4 + 1; k++) f[2 * k] = f[2 * k + 1] = (float)(k * step * scale);
+        break;
+    case UFOB_FILTER_RAMP_FROMREAL:
+        f[0] = f[1] = (float)(0.25 * scale);
+        for (uint32_t k = 1; k < width / 4 + 1; k++)
+            f[2 * k] = f[2 * k + 1] = (k % 2) ? (float)(-scale / ((double)k * k * M_PI * M_PI)) : 0.f;
+        break;
+    case UFOB_FILTER_BUTTERWORTH:
+        for (uint32_t k = 0; k < width / 4 + 1; k++) {
+            double fr = k * step;
+            f[2 * k] = f[2 * k + 1] = (float)(fr / (1.0 + pow(fr / cutoff, 2.0 * order)) * scale);
+        }
+        break;
+    case UFOB_FILTER_FARIS_BYER: {
+        const double pi_squared_tau = M_PI * M_PI * tau;
+        const double sin_theta_2 = -sin(theta) / 2;
+        const uint32_t padding = padding_value(width);
+        f[0] = 0;
+        for (uint32_t x = 1; x <= width / 2; x++)
+            if (x % 2 != 0) f[x] = (float)(1 / (pi_squared_tau * x));
+        for (uint32_t i = width / 2 + 1; i < width; i++) {
+            uint32_t x = width + 1 - i;
+            if (x % 2 != 0) f[padding - width - i - 1] = (float)(sin_theta_2 / ((double)x * x * pi_squared_tau));
+        }
+        break;
+    }
+    case UFOB_FILTER_HAMMING:
+        for (uint32_t k = 0; k < width / 4 + 1; k++) {
+            double fr = k * step;
+            f[2 * k] = f[2 * k + 1] =
+                fr < cutoff ? (float)(fr * (0.54 + 0.46 * cos(M_PI * fr / cutoff)) * scale) : 0.f;
+        }
+        break;
+    case UFOB_FILTER_BH3:
+        for (uint32_t k = 1; k < width / 4 + 1; k++) {
+            double fr = k * step;
+            f[2 * k] = f[2 * k + 1] =
+                (float)(fr * (0.42 + 0.5 * cos(fr * M_PI) + 0.08 * cos(2.0 * fr * M_PI)) * scale);
+        }
+        break;
+    default:
+        set_error("unknown filter type %d", p.filter);
+        return false;
+    }
+    // mirror_coefficients, src/ufo-filter-task.c:162-169
+    for (uint32_t k = width / 2 + 2; k < width; k += 2) {
+        f[k] = f[width - k];
+        f[k + 1] = f[width - k + 1];
+    }
+    return true;
+}
+
+// ------------------------------------------------------------ FP64 table kernels
+
+__global__ void k_twiddles(float2 *tw, uint32_t n)
+{
+    uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double s, c;
+    sincospi(-2.0 * (double)m / (double)n, &s, &c);
+    tw[m] = make_float2((float)c, (float)s);
+}
+
+// In-place forward DFT of the interleaved pairs (ramp-fromreal, src/ufo-filter-task.c:317-334),
+// FP64, direct summation over an exact index m = j*k mod n.
+__global__ void k_dft_pairs_fp64(const float *in, float *out, uint32_t n)
+{
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double re = 0.0, im = 0.0;
+    for (uint32_t j = 0; j < n; j++) {
+        uint32_t m = (uint32_t)(((uint64_t)j * k) & (n - 1));
+        double s, c;
+        sincospi(-2.0 * (double)m / (double)n, &s, &c);
+        double a = in[2 * j], b = in[2 * j + 1];
+        re += a * c - b * s;
+        im += a * s + b * c;
+    }
+    out[2 * k] = (float)re;
+    out[2 * k + 1] = (float)im;
+}
+
+// Symmetrised gains with the 1/N of the inverse transform folded in (exact: N is a power of two).
+__global__ void k_gains(const float *coeff, float2 *gains, uint32_t n)
+{
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > n / 2) return;
+    uint32_t m = (n - k) & (n - 1);
+    double inv = 1.0 / (double)n;
+    double gr = 0.5 * ((double)coeff[2 * k] + (double)coeff[2 * m]) * inv;
+    double gi = 0.5 * ((double)coeff[2 * k + 1] + (double)coeff[2 * m + 1]) * inv;
+    gains[k] = make_float2((float)gr, (float)gi);
+}
+
+ufob_status filter_plan_build(const ufob_filter_props &p, uint32_t nfft, FilterPlan &plan, cudaStream_t stream)
+{
+    if (plan.nfft == nfft && !plan.coeff.empty()) return UFOB_OK;
+    std::vector<float> c;
+    if (!build_filter_coefficients(p, nfft, c)) return UFOB_ERR_REQUISITION;
+    UFOB_TRY(plan.d_coeff.ensure(sizeof(float) * 2 * nfft));
+    UFOB_TRY(plan.d_gains.ensure(sizeof(float2) * (nfft / 2 + 1)));
+    UFOB_TRY(plan.d_twiddle.ensure(sizeof(float2) * nfft));
+    const int T = 256;
+    if (p.filter == UFOB_FILTER_RAMP_FROMREAL) {
+        DevBuf tmp;
+        UFOB_TRY(tmp.ensure(sizeof(float) * 2 * nfft));
+        UFOB_CUDA_TRY(cudaMemcpyAsync(tmp.ptr, c.data(), sizeof(float) * 2 * nfft, cudaMemcpyHostToDevice, stream));
+        k_dft_pairs_fp64<<<(nfft + T - 1) / T, T, 0, stream>>>(tmp.as<float>(), plan.d_coeff.as<float>(), nfft);
+        UFOB_CUDA_TRY(cudaGetLastError());
+        UFOB_CUDA_TRY(cudaMemcpyAsync(c.data(), plan.d_coeff.ptr, sizeof(float) * 2 * nfft, cudaMemcpyDeviceToHost,
+                                      stream));
+        UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
+    } else {
+        UFOB_CUDA_TRY(
+            cudaMemcpyAsync(plan.d_coeff.ptr, c.data(), sizeof(float) * 2 * nfft, cudaMemcpyHostToDevice, stream));
+    }
+    k_gains<<<(nfft / 2 + 1 + T - 1) / T, T, 0, stream>>>(plan.d_coeff.as<float>(), plan.d_gains.as<float2>(), nfft);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    k_twiddles<<<(nfft + T - 1) / T, T, 0, stream>>>(plan.d_twiddle.as<float2>(), nfft);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
+    plan.coeff.swap(c);
+    plan.nfft = nfft;
+    return UFOB_OK;
+}
+
+// ------------------------------------------------------------ fused row kernel
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// One Stockham pass of radix R over N points: src -> dst (both shared).
+// Twiddle for leg r of butterfly j in a sub-transform of size Ns*R is
+// w_N^(r * k * N / (Ns * R)) with k = j mod Ns (Govindaraju et al., SC'08).
+template <int R, bool INV>
+__device__ __forceinline__ void stockham_pass(const float2 *__restrict__ src, float2 *__restrict__ dst,
+                                              const float2 *__restrict__ tw, uint32_t N, uint32_t Ns, int twshift)
+{
+    const uint32_t nb = N / R;
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) {
+        const uint32_t k = j & (Ns - 1);
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) v[r] = src[j + r * nb];
+        if (Ns > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                float2 w = tw[(r * k) << twshift];
+                if (INV) w.y = -w.y;
+                v[r] = cmul(v[r], w);
+            }
+        }
+        if (R == 2) {
+            float2 a = v[0], b = v[1];
+            v[0] = cadd(a, b);
+            v[1] = csub(a, b);
+        } else {
+            float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+            float2 t2 = cadd(v[1], v[3]), d = csub(v[1], v[3]);
+            // forward: d * (-i) = (d.y, -d.x); inverse: d * i = (-d.y, d.x)
+            float2 t3 = INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
+            v[0] = cadd(t0, t2);
+            v[2] = csub(t0, t2);
+            v[1] = cadd(t1, t3);
+            v[3] = csub(t1, t3);
+        }
+        const uint32_t base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[base + r * Ns] = v[r];
+    }
+}
+
+// Full transform; returns the buffer holding the result.
+template <bool INV>
+__device__ float2 *fft_smem(float2 *a, float2 *b, const float2 *tw, uint32_t N, int log2N)
+{
+    uint32_t Ns = 1;
+    int l = log2N;
+    if (l & 1) {
+        stockham_pass<2, INV>(a, b, tw, N, Ns, l - 1);
+        __syncthreads();
+        float2 *t = a; a = b; b = t;
+        Ns = 2;
+        l -= 1;
+    }
+    while (l > 0) {
+        // twiddle index scale N / (Ns * 4) = 2^(log2N - log2(Ns) - 2)
+        int shift = log2N - (31 - __clz(Ns)) - 2;
+        stockham_pass<4, INV>(a, b, tw, N, Ns, shift);
+        __syncthreads();
+        float2 *t = a; a = b; b = t;
+        Ns *= 4;
+        l -= 2;
+    }
+    return a;
+}
+
+enum OutKind { OUT_F32 = 0, OUT_F16 = 1, OUT_BF16 = 2, OUT_F16_PAIRS = 3, OUT_BF16_PAIRS = 4 };
+
+template <int OUT>
+__device__ __forceinline__ void store_value(void *out, size_t idx, float v)
+{
+    if (OUT == OUT_F32) reinterpret_cast<float *>(out)[idx] = v;
+    if (OUT == OUT_F16) reinterpret_cast<__half *>(out)[idx] = __float2half_rn(v);
+    if (OUT == OUT_BF16) reinterpret_cast<__nv_bfloat16 *>(out)[idx] = __float2bfloat16_rn(v);
+}
+
+template <int OUT>
+__device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
+{
+    if (OUT == OUT_F16_PAIRS) {
+        __half2 h = __floats2half2_rn(lo, hi);
+        return *reinterpret_cast<uint32_t *>(&h);
+    } else {
+        __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+        return *reinterpret_cast<uint32_t *>(&h);
+    }
+}
+
+template <int OUT>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__restrict__ in, uint32_t width,
+                                                                uint32_t rows, uint32_t in_pitch,
+                                                                const float2 *__restrict__ g_tw,
+                                                                const float2 *__restrict__ g_gains, uint32_t N,
+                                                                int log2N, void *__restrict__ out, uint32_t out_w,
+                                                                uint32_t out_pitch)
+{
+    extern __shared__ float4 smem_f4[];
+    float2 *bufA = reinterpret_cast<float2 *>(smem_f4);
+    float2 *bufB = bufA + N;
+    float2 *tw = bufB + N;
+    float2 *gains = tw + N;
+
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g_tw[i];
+    for (uint32_t i = threadIdx.x; i <= N / 2; i += blockDim.x) gains[i] = g_gains[i];
+
+    const uint32_t npairs = (rows + 1) / 2;
+    for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
+        const uint32_t ra = 2 * pair, rb = 2 * pair + 1;
+        const bool hasb = rb < rows;
+        const float *pa = in + (size_t)ra * in_pitch;
+        const float *pb = in + (size_t)rb * in_pitch;
+        __syncthreads();  // previous pair's output reads of bufA/bufB are done
+        for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
+            float a = 0.f, b = 0.f;
+            if (n < width) {
+                a = __ldg(pa + n);
+                if (hasb) b = __ldg(pb + n);
+            }
+            bufA[n] = make_float2(a, b);
+        }
+        __syncthreads();
+        float2 *Z = fft_smem<false>(bufA, bufB, tw, N, log2N);
+        // separate, filter, recombine (pairs (k, N-k) are disjoint across threads)
+        for (uint32_t k = threadIdx.x; k <= N / 2; k += blockDim.x) {
+            const uint32_t m = (N - k) & (N - 1);
+            float2 zk = Z[k], zm = Z[m], g = gains[k];
+            float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
+            float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
+            ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
+            Z[k] = make_float2(ax - by, ay + bx);
+            if (m != k) Z[m] = make_float2(ax + by, bx - ay);
+        }
+        __syncthreads();
+        float2 *other = (Z == bufA) ? bufB : bufA;
+        float2 *X = fft_smem<true>(Z, other, tw, N, log2N);
+        if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
+            uint32_t *o = reinterpret_cast<uint32_t *>(out);
+            for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
+                float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
+                float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
+                o[(size_t)ra * out_pitch + j] = pack_pair<OUT>(lo.x, hi.x);
+                if (hasb) o[(size_t)rb * out_pitch + j] = pack_pair<OUT>(lo.y, hi.y);
+            }
+        } else {
+            for (uint32_t n = threadIdx.x; n < out_w; n += blockDim.x) {
+                float2 v = X[n];
+                store_value<OUT>(out, (size_t)ra * out_pitch + n, v.x);
+                if (hasb) store_value<OUT>(out, (size_t)rb * out_pitch + n, v.y);
+            }
+        }
+    }
+}
+
+template <int OUT>
+static ufob_status launch_rows(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
+                               uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s)
+{
+    const uint32_t N = plan.nfft;
+    const size_t smem = sizeof(float2) * (3 * (size_t)N + N / 2 + 1);
+    static bool attr_set[16] = {};
+    int log2N = ilog2(N);
+    if (!attr_set[log2N]) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_filter_rows<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(sizeof(float2) * (3 * (size_t)kMaxFusedFFT + kMaxFusedFFT / 2 + 1))));
+        attr_set[log2N] = true;
+    }
+    int per_sm = 0;
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_rows<OUT>, kFilterThreads, smem));
+    if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);
+    const uint32_t npairs = (rows + 1) / 2;
+    uint32_t grid = (uint32_t)num_sms() * (uint32_t)per_sm * 4;
+    if (grid > npairs) grid = npairs;
+    if (grid == 0) return UFOB_OK;
+    k_filter_rows<OUT><<<grid, kFilterThreads, smem, s>>>(d_in, width, rows, in_pitch, plan.d_twiddle.as<float2>(),
+                                                          plan.d_gains.as<float2>(), N, log2N, d_out, out_w,
+                                                          out_pitch);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
+                               uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
+                               uint32_t out_w, uint32_t out_pitch, cudaStream_t stream)
+{
+    const uint32_t N = plan.nfft;
+    if (N > kMaxFusedFFT || N < 4)
+        return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u outside the supported range [4, %u]", N, kMaxFusedFFT);
+    if (width > N) return fail(UFOB_ERR_INVALID, "filter: input width %u exceeds FFT width %u", width, N);
+    if (out_w > N) return fail(UFOB_ERR_INVALID, "filter: crop width %u exceeds FFT width %u", out_w, N);
+    if (in_pitch < width) return fail(UFOB_ERR_INVALID, "filter: input pitch %u < width %u", in_pitch, width);
+    if (out_layout == UFOB_LAYOUT_PAIRS) {
+        if (out_pitch < out_w + 1) return fail(UFOB_ERR_INVALID, "filter: pair pitch %u < crop width + 1", out_pitch);
+        if (out_dtype == UFOB_F16) return launch_rows<OUT_F16_PAIRS>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+        if (out_dtype == UFOB_BF16) return launch_rows<OUT_BF16_PAIRS>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+        return fail(UFOB_ERR_INVALID, "filter: the pair layout needs F16 or BF16 output");
+    }
+    if (out_pitch < out_w) return fail(UFOB_ERR_INVALID, "filter: output pitch %u < crop width %u", out_pitch, out_w);
+    switch (out_dtype) {
+    case UFOB_F32: return launch_rows<OUT_F32>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+    case UFOB_F16: return launch_rows<OUT_F16>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+    case UFOB_BF16: return launch_rows<OUT_BF16>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+    default: return fail(UFOB_ERR_INVALID, "filter: unsupported output dtype %d", (int)out_dtype);
+    }
+}
+
+// The reference `filter` kernel alone (filter.cl:20-29): out[y][x] = in[y][x] * coeff[x].
+__global__ void k_filter_spectrum(const float *__restrict__ coeff, const float *__restrict__ in,
+                                  float *__restrict__ out, uint32_t width2, uint32_t rows)
+{
+    size_t n = (size_t)width2 * rows;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = in[i] * __ldg(coeff + (i % width2));
+}
+
+ufob_status filter_spectrum_launch(const float *d_coeff, const float *d_in, float *d_out, uint32_t width2,
+                                   uint32_t rows, cudaStream_t stream)
+{
+    size_t n = (size_t)width2 * rows;
+    if (!n) return UFOB_OK;
+    uint32_t grid = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)num_sms() * 16);
+    k_filter_spectrum<<<grid, 256, 0, stream>>>(d_coeff, d_in, d_out, width2, rows);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+}  // namespace ufob

@@ -1,0 +1,102 @@
+// Internal declarations shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ufob.h"
+
+namespace ufob {
+
+// Thread-local error text returned by ufob_last_error().
+void set_error(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
+ufob_status fail(ufob_status st, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+ufob_status cuda_fail(cudaError_t e, const char *what);
+ufob_status ensure_device();  // UFOB_ERR_CUDA unless an sm_100 device is current
+int num_sms();
+
+#define UFOB_CUDA_TRY(expr)                                       \
+    do {                                                          \
+        cudaError_t _e = (expr);                                  \
+        if (_e != cudaSuccess) return ::ufob::cuda_fail(_e, #expr); \
+    } while (0)
+
+#define UFOB_TRY(expr)                        \
+    do {                                      \
+        ufob_status _s = (expr);              \
+        if (_s != UFOB_OK) return _s;         \
+    } while (0)
+
+// Device buffer owned by an engine object.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    ufob_status ensure(size_t n);  // grow to at least n bytes (contents not kept)
+    template <typename T> T *as() const { return reinterpret_cast<T *>(ptr); }
+};
+
+// Device error word: kernels with bounded waits record a code here instead of
+// trapping.  0 = no error.
+int *device_error_word();
+ufob_status check_device_error_word(cudaStream_t stream);
+
+inline uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
+inline bool is_pow2(uint64_t v) { return v && !(v & (v - 1)); }
+inline int ilog2(uint64_t v) {
+    int l = 0;
+    while ((1ull << l) < v) l++;
+    return l;
+}
+
+// ---------------------------------------------------------------- filter stage
+struct FilterPlan {
+    uint32_t nfft = 0;
+    std::vector<float> coeff;  // 2*nfft interleaved coefficients, as the reference uploads
+    DevBuf d_coeff;            // same on the device (float)
+    DevBuf d_gains;            // float2 [nfft/2 + 1]: symmetrised per-bin gains
+    DevBuf d_twiddle;          // float2 [nfft]: exp(-2 pi i m / nfft), FP64-computed
+};
+
+// Host restatement of the reference's coefficient builders (before the
+// ramp-fromreal transform).  Returns false and sets the error on bad width.
+bool build_filter_coefficients(const ufob_filter_props &p, uint32_t nfft, std::vector<float> &coeff);
+ufob_status filter_plan_build(const ufob_filter_props &p, uint32_t nfft, FilterPlan &plan, cudaStream_t stream);
+ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
+                               uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
+                               uint32_t out_w, uint32_t out_pitch, cudaStream_t stream);
+ufob_status filter_spectrum_launch(const float *d_coeff, const float *d_in, float *d_out, uint32_t width2,
+                                   uint32_t rows, cudaStream_t stream);
+
+// ------------------------------------------------------- parallel backprojection
+struct BPGeometry {
+    uint32_t W = 0, P = 0, nz = 0;  // sinogram width, rows used, slices
+    uint32_t roi_x = 0, roi_y = 0, roi_w = 0, roi_h = 0;
+    float axis = 0.f;
+    float norm = 0.f;              // pi / P
+    const float2 *d_sincos = nullptr;  // [P] (sin, cos) of the angles actually used
+};
+
+// sin/cos of angle_offset + (lut_offset + p) * step for p < P, in FP64 on the device.
+ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *d_out,
+                                cudaStream_t stream);
+
+enum SinoKind { SINO_F32 = 0, SINO_F16_PAIRS = 1, SINO_BF16_PAIRS = 2 };
+
+ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
+                             uint64_t slice_pitch, float *d_out, bool kahan, int tile, cudaStream_t stream);
+ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t pitch, uint64_t slice_pitch,
+                              float *d_out, cudaStream_t stream);
+
+}  // namespace ufob

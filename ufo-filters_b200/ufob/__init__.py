@@ -1,0 +1,439 @@
+"""Python binding of the B200 FBP engine (ctypes over ``include/ufob.h``).
+
+The task classes mirror the ufo-filters tasks they replace: they are created by
+name (``get_task("filter")``, like ``Ufo.PluginManager().get_task``), take the
+reference's properties through ``task.props.<name>`` (dashes become
+underscores, as in PyGObject) and run on device tensors.  Device memory is held
+in torch CUDA tensors; every computation happens in the engine's own CUDA
+kernels inside ``libufob.so``.  There is no CPU path: if the library or a
+usable sm_100 GPU is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+__all__ = ["lib", "UfobError", "get_task", "FilterTask", "BackprojectTask", "FBP", "GeneralBackprojectTask",
+           "Batch", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libufob.so")
+
+OK, ERR_INVALID, ERR_SETUP, ERR_REQUISITION, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
+F32, F16, BF16, F64, U8, U16, U32 = range(7)
+ROWS, PAIRS = 0, 1
+FILTERS = ["ramp", "ramp-fromreal", "butterworth", "faris-byer", "hamming", "bh3"]
+DTYPES = {"f32": F32, "float": F32, "f16": F16, "half": F16, "bf16": BF16, "f64": F64, "double": F64,
+          "u8": U8, "uchar": U8, "u16": U16, "ushort": U16, "u32": U32, "uint": U32}
+
+_lib = None
+
+
+class UfobError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s (status %d)" % (message, status))
+        self.status = status
+
+
+class FilterProps(ctypes.Structure):
+    _fields_ = [("filter", ctypes.c_int), ("cutoff", ctypes.c_float), ("order", ctypes.c_float),
+                ("tau", ctypes.c_float), ("theta", ctypes.c_float), ("scale", ctypes.c_float),
+                ("size_x", ctypes.c_uint32), ("crop_width", ctypes.c_uint32)]
+
+
+class BPProps(ctypes.Structure):
+    _fields_ = [("num_projections", ctypes.c_uint32), ("offset", ctypes.c_uint32), ("axis_pos", ctypes.c_double),
+                ("angle_step", ctypes.c_double), ("angle_offset", ctypes.c_double), ("mode", ctypes.c_int),
+                ("roi_x", ctypes.c_uint32), ("roi_y", ctypes.c_uint32), ("roi_width", ctypes.c_uint32),
+                ("roi_height", ctypes.c_uint32), ("compensated", ctypes.c_int), ("tile", ctypes.c_int)]
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("d_sino", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("axis_pos", ctypes.c_double), ("angle_step", ctypes.c_double),
+                ("angle_offset", ctypes.c_double)]
+
+
+def lib():
+    """Load libufob.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libufob.so not found at %s: build it with `python ufo-filters_b200/build.py`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64, d, i, cs = (ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_int,
+                                  ctypes.c_char_p)
+        pu32 = ctypes.POINTER(ctypes.c_uint32)
+        sig = {
+            "ufob_last_error": ([], cs),
+            "ufob_status_string": ([i], cs),
+            "ufob_device_check": ([ctypes.POINTER(i), ctypes.POINTER(i), ctypes.POINTER(i)], i),
+            "ufob_device_status": ([], i),
+            "ufob_filter_props_init": ([ctypes.POINTER(FilterProps)], None),
+            "ufob_filter_create": ([ctypes.POINTER(FilterProps), ctypes.POINTER(vp)], i),
+            "ufob_filter_set_property": ([vp, cs, d], i),
+            "ufob_filter_set_property_string": ([vp, cs, cs], i),
+            "ufob_filter_get_requisition": ([vp, u32, u32, pu32, pu32], i),
+            "ufob_filter_run": ([vp, vp, u32, u32, u32, vp, i, i, u32, vp], i),
+            "ufob_filter_coefficients": ([vp, u32, vp, u32], i),
+            "ufob_filter_apply_spectrum": ([vp, vp, vp, u32, u32, vp], i),
+            "ufob_filter_destroy": ([vp], None),
+            "ufob_bp_props_init": ([ctypes.POINTER(BPProps)], None),
+            "ufob_backproject_create": ([ctypes.POINTER(BPProps), ctypes.POINTER(vp)], i),
+            "ufob_backproject_set_property": ([vp, cs, d], i),
+            "ufob_backproject_set_property_string": ([vp, cs, cs], i),
+            "ufob_backproject_get_requisition": ([vp, u32, u32, pu32, pu32], i),
+            "ufob_backproject_run": ([vp, vp, i, i, u32, u32, u32, u32, u64, vp, vp], i),
+            "ufob_backproject_destroy": ([vp], None),
+            "ufob_fbp_create": ([ctypes.POINTER(FilterProps), ctypes.POINTER(BPProps), i, ctypes.POINTER(vp)], i),
+            "ufob_fbp_run": ([vp, vp, u32, u32, u32, vp, vp], i),
+            "ufob_fbp_run_host": ([vp, vp, u32, u32, u32, vp, u32], i),
+            "ufob_fbp_get_requisition": ([vp, u32, u32, pu32, pu32], i),
+            "ufob_fbp_destroy": ([vp], None),
+            "ufob_gbp_create": ([ctypes.POINTER(vp)], i),
+            "ufob_gbp_set_property": ([vp, cs, d], i),
+            "ufob_gbp_set_property_string": ([vp, cs, cs], i),
+            "ufob_gbp_set_array": ([vp, cs, vp, u32], i),
+            "ufob_gbp_setup": ([vp], i),
+            "ufob_gbp_get_requisition": ([vp, u32, u32, pu32, pu32, pu32], i),
+            "ufob_gbp_run": ([vp, vp, u32, u32, vp, vp], i),
+            "ufob_gbp_process": ([vp, vp, u32, u32, vp], i),
+            "ufob_gbp_generate": ([vp, vp, u32, vp], i),
+            "ufob_gbp_destroy": ([vp], None),
+            "ufob_batch_create": ([ctypes.POINTER(FilterProps), i, ctypes.POINTER(vp)], i),
+            "ufob_batch_run": ([vp, ctypes.POINTER(Job), u32, vp], i),
+            "ufob_batch_destroy": ([vp], None),
+            "ufob_phantom_sinogram": ([vp, u32, u32, u32, d, d, d, vp, vp], i),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != OK:
+        raise UfobError(status, lib().ufob_last_error().decode())
+    return status
+
+
+def _ptr(t):
+    """Device pointer of a CUDA tensor (or an int address)."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    return t.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream if isinstance(stream, int) else stream.cuda_stream
+
+
+class _Props:
+    """Attribute-style property access: props.axis_pos = 255.5 -> set_property('axis-pos', 255.5)."""
+
+    def __init__(self, task):
+        object.__setattr__(self, "_task", task)
+
+    def __setattr__(self, name, value):
+        self._task.set_property(name.replace("_", "-"), value)
+
+    def __getattr__(self, name):
+        return self._task.get_property(name.replace("_", "-"))
+
+
+class _Task:
+    _set_num = None
+    _set_str = None
+
+    def __init__(self):
+        self.props = _Props(self)
+        self._values = {}
+
+    def set_property(self, name, value):
+        if isinstance(value, str):
+            check(self._set_str(self._h, name.encode(), value.encode()))
+        else:
+            check(self._set_num(self._h, name.encode(), float(value)))
+        self._values[name] = value
+
+    def get_property(self, name):
+        if name in self._values:
+            return self._values[name]
+        raise AttributeError(name)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._destroy(h)
+            self._h = None
+
+
+class FilterTask(_Task):
+    """Fused ``fft ! filter ! ifft`` (ramp filter along detector rows).
+
+    Properties: filter, cutoff, order, tau, theta, scale (filter task),
+    size-x (fft task), crop-width (ifft task)."""
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_filter_create(None, ctypes.byref(h)))
+        self._h = h
+        self._set_num, self._set_str, self._destroy = (L.ufob_filter_set_property, L.ufob_filter_set_property_string,
+                                                       L.ufob_filter_destroy)
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def get_requisition(self, width, height):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_filter_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h)))
+        return w.value, h.value
+
+    def coefficients(self, width):
+        import numpy as np
+        w, _ = self.get_requisition(width, 1)
+        n = 2 * (self.get_property("size-x") if self._values.get("size-x") else width)
+        out = np.zeros(n, dtype=np.float32)
+        check(lib().ufob_filter_coefficients(self._h, width, out.ctypes.data, n))
+        return out
+
+    def process(self, sino, dtype=F32, layout=ROWS, out=None, stream=None):
+        """Filter the rows of a float32 CUDA tensor [..., H, W]; returns [..., H, crop]
+        (or [..., H, pair_pitch] int32 pairs for layout=PAIRS)."""
+        import torch
+        if sino.dtype != torch.float32 or not sino.is_cuda:
+            raise ValueError("sinogram must be a float32 CUDA tensor")
+        sino = sino.contiguous()
+        W = sino.shape[-1]
+        rows = sino.numel() // W
+        cw, _ = self.get_requisition(W, 1)
+        dt = DTYPES.get(dtype, dtype) if isinstance(dtype, str) else dtype
+        if layout == PAIRS:
+            pitch = (cw + 1 + 3) // 4 * 4
+            shape = tuple(sino.shape[:-1]) + (pitch,)
+            out = torch.empty(shape, dtype=torch.int32, device=sino.device) if out is None else out
+        else:
+            pitch = cw
+            tdt = {F32: torch.float32, F16: torch.float16, BF16: torch.bfloat16}[dt]
+            shape = tuple(sino.shape[:-1]) + (cw,)
+            out = torch.empty(shape, dtype=tdt, device=sino.device) if out is None else out
+        check(lib().ufob_filter_run(self._h, _ptr(sino), W, rows, W, _ptr(out), dt, layout, pitch, _stream(stream)))
+        return out
+
+    def apply_spectrum(self, spec, stream=None):
+        """The reference ``filter`` task alone on complex-interleaved rows [..., 2*N]."""
+        import torch
+        spec = spec.contiguous()
+        out = torch.empty_like(spec)
+        w2 = spec.shape[-1]
+        check(lib().ufob_filter_apply_spectrum(self._h, _ptr(spec), _ptr(out), w2, spec.numel() // w2,
+                                               _stream(stream)))
+        return out
+
+
+class BackprojectTask(_Task):
+    """Parallel-beam ``backproject``.
+
+    Properties: num-projections, offset, axis-pos, angle-step, angle-offset,
+    mode (nearest|texture), roi-x, roi-y, roi-width, roi-height; engine
+    extensions: compensated, tile."""
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_backproject_create(None, ctypes.byref(h)))
+        self._h = h
+        self._set_num, self._set_str, self._destroy = (L.ufob_backproject_set_property,
+                                                       L.ufob_backproject_set_property_string,
+                                                       L.ufob_backproject_destroy)
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def get_requisition(self, width, height):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_backproject_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h)))
+        return w.value, h.value
+
+    def process(self, sino, dtype=F32, layout=ROWS, width=None, out=None, stream=None):
+        """Backproject [H, W] or [Z, H, W] float32 sinograms (or F16/BF16 pairs
+        from FilterTask.process(layout=PAIRS), then pass ``width``)."""
+        import torch
+        squeeze = sino.dim() == 2
+        s3 = sino.unsqueeze(0) if squeeze else sino
+        s3 = s3.contiguous()
+        Z, H, pitch = s3.shape
+        W = pitch if layout == ROWS else width
+        if W is None:
+            raise ValueError("pass width= for the pair layout")
+        ow, oh = self.get_requisition(W, H)
+        out = torch.empty((Z, oh, ow), dtype=torch.float32, device=s3.device) if out is None else out
+        check(lib().ufob_backproject_run(self._h, _ptr(s3), dtype, layout, W, H, Z, pitch, pitch * H, _ptr(out),
+                                         _stream(stream)))
+        return out[0] if squeeze else out
+
+
+class FBP:
+    """``fft ! filter ! ifft ! backproject`` for a sinogram stack, one call.
+
+    storage: filtered-sinogram storage type (F32, F16 or BF16)."""
+
+    def __init__(self, filter_props=None, bp_props=None, storage=F32):
+        L = lib()
+        fp = FilterProps()
+        L.ufob_filter_props_init(ctypes.byref(fp))
+        for k, v in (filter_props or {}).items():
+            k = k.replace("-", "_")
+            if k == "filter" and isinstance(v, str):
+                v = FILTERS.index(v)
+            setattr(fp, k, v)
+        bpp = BPProps()
+        L.ufob_bp_props_init(ctypes.byref(bpp))
+        for k, v in (bp_props or {}).items():
+            k = k.replace("-", "_")
+            if k == "mode" and isinstance(v, str):
+                v = {"nearest": 0, "texture": 1}[v]
+            setattr(bpp, k, v)
+        h = ctypes.c_void_p()
+        check(L.ufob_fbp_create(ctypes.byref(fp), ctypes.byref(bpp), DTYPES.get(storage, storage)
+                                if isinstance(storage, str) else storage, ctypes.byref(h)))
+        self._h = h
+
+    def get_requisition(self, width, height):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_fbp_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h)))
+        return w.value, h.value
+
+    def process(self, sino, out=None, stream=None):
+        import torch
+        squeeze = sino.dim() == 2
+        s3 = (sino.unsqueeze(0) if squeeze else sino).contiguous()
+        Z, H, W = s3.shape
+        ow, oh = self.get_requisition(W, H)
+        out = torch.empty((Z, oh, ow), dtype=torch.float32, device=s3.device) if out is None else out
+        check(lib().ufob_fbp_run(self._h, _ptr(s3), W, H, Z, _ptr(out), _stream(stream)))
+        return out[0] if squeeze else out
+
+    def process_host(self, sino, out=None, slices_per_chunk=32):
+        """Host tensors/arrays in, host out; copies overlap compute inside the engine."""
+        import torch
+        Z, H, W = sino.shape
+        ow, oh = self.get_requisition(W, H)
+        if out is None:
+            out = torch.empty((Z, oh, ow), dtype=torch.float32)
+        check(lib().ufob_fbp_run_host(self._h, sino.data_ptr(), W, H, Z, out.data_ptr(), slices_per_chunk))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ufob_fbp_destroy(self._h)
+            self._h = None
+
+
+class GeneralBackprojectTask(_Task):
+    """``general-backproject``: parallel, cone and laminography volumes."""
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_gbp_create(ctypes.byref(h)))
+        self._h = h
+        self._set_num, self._set_str, self._destroy = (L.ufob_gbp_set_property, L.ufob_gbp_set_property_string,
+                                                       L.ufob_gbp_destroy)
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def set_property(self, name, value):
+        if isinstance(value, (list, tuple)) or hasattr(value, "__len__") and not isinstance(value, str):
+            import numpy as np
+            arr = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+            check(lib().ufob_gbp_set_array(self._h, name.encode(), arr.ctypes.data, arr.size))
+            self._values[name] = arr
+        else:
+            super().set_property(name, value)
+
+    def setup(self):
+        check(lib().ufob_gbp_setup(self._h))
+
+    def get_requisition(self, width, height):
+        w, h, n = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_gbp_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h),
+                                             ctypes.byref(n)))
+        return w.value, h.value, n.value
+
+    def process(self, proj, out=None, stream=None, dtype=None):
+        import torch
+        proj = proj.contiguous()
+        n, H, W = proj.shape
+        self.setup()
+        ow, oh, ns = self.get_requisition(W, H)
+        st = self._values.get("store-type", "float")
+        tdt = {"half": torch.float16, "float": torch.float32, "double": torch.float64, "uchar": torch.uint8,
+               "ushort": torch.uint16, "uint": torch.uint32}[st]
+        out = torch.empty((ns, oh, ow), dtype=tdt, device=proj.device) if out is None else out
+        check(lib().ufob_gbp_run(self._h, _ptr(proj), W, H, _ptr(out), _stream(stream)))
+        return out
+
+
+class Batch:
+    """Uneven batch of parallel-beam FBP jobs in one persistent launch."""
+
+    def __init__(self, filter_props=None, storage=F32):
+        L = lib()
+        fp = FilterProps()
+        L.ufob_filter_props_init(ctypes.byref(fp))
+        for k, v in (filter_props or {}).items():
+            setattr(fp, k.replace("-", "_"), v)
+        h = ctypes.c_void_p()
+        check(L.ufob_batch_create(ctypes.byref(fp), storage, ctypes.byref(h)))
+        self._h = h
+
+    def run(self, jobs, stream=None):
+        arr = (Job * len(jobs))()
+        for i, j in enumerate(jobs):
+            arr[i] = Job(_ptr(j["sino"]), _ptr(j["out"]), j["sino"].shape[-1], j["sino"].shape[-2],
+                         j.get("axis_pos", -1.0), j.get("angle_step", -1.0), j.get("angle_offset", 0.0))
+        check(lib().ufob_batch_run(self._h, arr, len(jobs), _stream(stream)))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ufob_batch_destroy(self._h)
+            self._h = None
+
+
+def get_task(name, **props):
+    """Create a task by its ufo-filters name."""
+    table = {"filter": FilterTask, "backproject": BackprojectTask, "general-backproject": GeneralBackprojectTask}
+    if name not in table:
+        raise KeyError("no task named %r (available: %s)" % (name, ", ".join(sorted(table))))
+    return table[name](**props)
+
+
+def device_status():
+    check(lib().ufob_device_status())
+
+
+def phantom_sinogram(ellipses, width, n_angles, angle_step=None, axis=None, scale=None, out=None, stream=None):
+    """Analytic ellipse sinogram [n_angles, width] computed on the device."""
+    import numpy as np
+    import torch
+    ell = np.ascontiguousarray(ellipses, dtype=np.float64)
+    step = math.pi / n_angles if angle_step is None else angle_step
+    axis = width / 2.0 if axis is None else axis
+    scale = width / 2.0 if scale is None else scale
+    out = torch.empty((n_angles, width), dtype=torch.float32, device="cuda") if out is None else out
+    check(lib().ufob_phantom_sinogram(ell.ctypes.data, len(ell), width, n_angles, step, axis, scale, _ptr(out),
+                                      _stream(stream)))
+    return out
