@@ -237,6 +237,19 @@ ufob_status ufob_phantom_sinogram(const double *h_ellipses, uint32_t n_ellipses,
                                   uint32_t n_angles, double angle_step, double axis, double scale, float *d_sino,
                                   void *stream);
 
+/* Stack [nz][n_angles][width] of sinograms of an ellipsoid phantom (rows cx,
+ * cy, cz, a, b, c, phi, rho; at most 64), slice z cutting the phantom at height
+ * (z + 0.5 - nz/2) / scale. */
+ufob_status ufob_phantom_stack(const double *h_ellipsoids, uint32_t n, uint32_t width, uint32_t n_angles,
+                               uint32_t nslices, double angle_step, double axis, double scale, float *d_sino,
+                               void *stream);
+/* Number of engine kernels launched by this process so far. */
+uint64_t ufob_launch_count(void);
+/* Sustained shared-memory load bandwidth (GB/s, 32-bit conflict-free loads)
+ * and FP32 FMA throughput (TFLOP/s) of the current device, measured by two
+ * short micro-kernels: the on-chip ceilings of voxel-driven backprojection. */
+ufob_status ufob_measure_peaks(double *smem_gbs, double *fp32_tflops);
+
 #ifdef __cplusplus
 }
 #endif

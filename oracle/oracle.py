@@ -352,6 +352,32 @@ def random_ellipses(seed, n=10, semi=(0.05, 0.4), density=(-0.5, 1.0)):
     return np.ascontiguousarray(ell, dtype=np.float64)
 
 
+def random_ellipsoids(seed, n=50, semi=(0.05, 0.4), density=(-0.5, 1.0)):
+    """Rows (cx, cy, cz, a, b, c, phi, rho): centres uniform in the unit ball,
+    semi-axes uniform in ``semi``, rotation about z uniform in [0, pi),
+    densities uniform in ``density``."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    v *= rng.uniform(0, 1, (n, 1)) ** (1.0 / 3.0)
+    ell = np.concatenate([v, rng.uniform(*semi, (n, 3)), rng.uniform(0, math.pi, (n, 1)),
+                          rng.uniform(*density, (n, 1))], axis=1)
+    return np.ascontiguousarray(ell, dtype=np.float64)
+
+
+def ellipsoid_slice_ellipses(ell3, z, nz, scale):
+    """Ellipses (cx, cy, a, b, phi, rho) that slice z of an nz-slice stack cuts
+    from the ellipsoids (slice centre height (z + 0.5 - nz/2) / scale)."""
+    zu = (z + 0.5 - 0.5 * nz) / scale
+    rows = []
+    for q in ell3:
+        dz = (zu - q[2]) / q[5]
+        if dz * dz < 1.0:
+            f = math.sqrt(1.0 - dz * dz)
+            rows.append([q[0], q[1], q[3] * f, q[4] * f, q[6], q[7]])
+    return np.ascontiguousarray(np.array(rows, dtype=np.float64).reshape(-1, 6))
+
+
 def ellipse_sinogram(ell, width, angles, axis=None, scale=None):
     """Analytic parallel-beam sinogram [P, width] in pixel-length units."""
     axis = width / 2.0 if axis is None else axis

@@ -150,6 +150,7 @@ ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_o
     if (!P) return UFOB_OK;
     k_sincos<<<(P + 255) / 256, 256, 0, stream>>>(angle_offset, step, lut_offset, P, d_out);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 
@@ -174,8 +175,13 @@ struct BPShape {
     // one guard element on each side and 3 for the 16-byte TMA alignment
     static constexpr int kSpan = (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
     static constexpr int kWin = ((kSpan + 2 + 2 + 3) + 3) / 4 * 4;
-    static constexpr int kStageElems = A * ZT * kWin;
-    static constexpr size_t kSmem = (size_t)S * kStageElems * 4 + (size_t)S * A * 4 + (size_t)S * 8 + 128;
+    // each angle's box lands at a 128-byte aligned shared address (TMA destination rule)
+    static constexpr int kAngleStride = (ZT * kWin + 31) / 32 * 32;
+    static constexpr int kStageElems = A * kAngleStride;
+    static constexpr size_t kDataBytes = (size_t)S * kStageElems * 4;
+    static constexpr size_t kWinOffset = kDataBytes;
+    static constexpr size_t kBarOffset = (kWinOffset + (size_t)S * A * 4 + 7) / 8 * 8;
+    static constexpr size_t kSmem = kBarOffset + (size_t)S * 8 + 128;  // +128: manual base alignment
 };
 
 template <int KIND>
@@ -197,10 +203,13 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
     constexpr int RY = Sh::kRY;
     constexpr int YSTEP = 256 / TX;
     constexpr bool PAIRS = KIND != SINO_F32;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    uint32_t *data = reinterpret_cast<uint32_t *>(smem_raw);  // [S][A][ZT][WIN]
-    int *win = reinterpret_cast<int *>(smem_raw + (size_t)S * Sh::kStageElems * 4);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + (size_t)S * Sh::kStageElems * 4 + (size_t)S * A * 4);
+    constexpr int ASTR = Sh::kAngleStride;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem_raw =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
+    uint32_t *data = reinterpret_cast<uint32_t *>(smem_raw);  // [S][A][ASTR], angle box = [ZT][WIN]
+    int *win = reinterpret_cast<int *>(smem_raw + Sh::kWinOffset);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + Sh::kBarOffset);
 
     const int tid = threadIdx.x;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * ZT;
@@ -234,7 +243,7 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
             e = max(min(e, 1 << 24), -(1 << 24));
             const int xs = e & ~3;  // 16-byte aligned TMA x coordinate (floor for negatives)
             win[slot * A + a] = xs;
-            tma_load_3d(data + (size_t)(slot * A + a) * ZT * WIN, &map, &full[slot], xs, p0 + a, z0);
+            tma_load_3d(data + (size_t)(slot * A + a) * ASTR, &map, &full[slot], xs, p0 + a, z0);
         }
     };
 
@@ -265,7 +274,7 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
         const bool ok = mbar_wait_bounded(&full[slot], parity, kWaitLimitNs);
         const int p0 = blk * A;
         const int nval = min(A, (int)P - p0);
-        const uint32_t *sdata = data + (size_t)slot * A * ZT * WIN;
+        const uint32_t *sdata = data + (size_t)slot * A * ASTR;
 
         float part[RY][ZT];
 #pragma unroll
@@ -279,7 +288,7 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
                 const float2 sc = __ldg(&args.sincos[p0 + a]);
                 const int xs = win[slot * A + a];
                 const float t = fmaf(bx, sc.y, eoff - (float)xs);
-                const uint32_t *row = sdata + a * ZT * WIN;
+                const uint32_t *row = sdata + a * ASTR;
 #pragma unroll
                 for (int j = 0; j < RY; j++) {
                     const float vv = fmaf(by[j], sc.x, t);  // element coordinate - 0.5
@@ -368,8 +377,8 @@ __global__ void k_bp_nearest(const float *__restrict__ sino, uint32_t W, uint32_
     float sum = 0.f;
     for (uint32_t p = 0; p < P; p++) {
         const float2 sc = __ldg(&sincos[p]);
-        const float h = axis + bx * sc.y + by * sc.x;
-        const float fi = (float)(p * roi_w) + h;
+        const float h = fmaf(by, sc.x, fmaf(bx, sc.y, axis));  // axis + bx*cos + by*sin
+        const float fi = __fadd_rn((float)(p * roi_w), h);
         const long long k = (long long)fi;
         if (k >= 0 && k < (long long)W * P) {
             // element k of the flat [P][W] sinogram, honouring the caller's pitch
@@ -388,6 +397,7 @@ ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t
     k_bp_nearest<<<grd, blk, 0, stream>>>(d_sino, g.W, g.P, pitch, slice_pitch, g.nz, g.d_sincos, g.roi_x, g.roi_y,
                                           g.roi_w, g.roi_h, g.axis, g.norm, d_out);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 
@@ -421,6 +431,7 @@ static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32
     dim3 grid((g.roi_w + TX - 1) / TX, (g.roi_h + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
     kern<<<grid, Sh::kThreads, Sh::kSmem, stream>>>(map, a);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <strings.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <string>
 
@@ -59,6 +60,9 @@ ufob_status DevBuf::ensure(size_t n)
 }
 
 static int g_num_sms = 0;
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 ufob_status ensure_device()
 {
@@ -637,6 +641,8 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
 }
 
 extern "C" void ufob_fbp_destroy(ufob_fbp *x) { delete x; }
+
+extern "C" uint64_t ufob_launch_count(void) { return g_launches.load(); }
 
 extern "C" ufob_status ufob_device_status(void)
 {

@@ -166,6 +166,7 @@ ufob_status filter_plan_build(const ufob_filter_props &p, uint32_t nfft, FilterP
         UFOB_CUDA_TRY(cudaMemcpyAsync(tmp.ptr, c.data(), sizeof(float) * 2 * nfft, cudaMemcpyHostToDevice, stream));
         k_dft_pairs_fp64<<<(nfft + T - 1) / T, T, 0, stream>>>(tmp.as<float>(), plan.d_coeff.as<float>(), nfft);
         UFOB_CUDA_TRY(cudaGetLastError());
+        note_launch();
         UFOB_CUDA_TRY(cudaMemcpyAsync(c.data(), plan.d_coeff.ptr, sizeof(float) * 2 * nfft, cudaMemcpyDeviceToHost,
                                       stream));
         UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -175,8 +176,10 @@ ufob_status filter_plan_build(const ufob_filter_props &p, uint32_t nfft, FilterP
     }
     k_gains<<<(nfft / 2 + 1 + T - 1) / T, T, 0, stream>>>(plan.d_coeff.as<float>(), plan.d_gains.as<float2>(), nfft);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     k_twiddles<<<(nfft + T - 1) / T, T, 0, stream>>>(plan.d_twiddle.as<float2>(), nfft);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
     plan.coeff.swap(c);
     plan.nfft = nfft;
@@ -369,6 +372,7 @@ static ufob_status launch_rows(const FilterPlan &plan, const float *d_in, uint32
                                                           plan.d_gains.as<float2>(), N, log2N, d_out, out_w,
                                                           out_pitch);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 
@@ -414,6 +418,7 @@ ufob_status filter_spectrum_launch(const float *d_coeff, const float *d_in, floa
     uint32_t grid = (uint32_t)std::min<size_t>((n + 255) / 256, (size_t)num_sms() * 16);
     k_filter_spectrum<<<grid, 256, 0, stream>>>(d_coeff, d_in, d_out, width2, rows);
     UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 

@@ -17,6 +17,7 @@ ufob_status fail(ufob_status st, const char *fmt, ...) __attribute__((format(pri
 ufob_status cuda_fail(cudaError_t e, const char *what);
 ufob_status ensure_device();  // UFOB_ERR_CUDA unless an sm_100 device is current
 int num_sms();
+void note_launch(uint64_t n = 1);  // count kernels launched (ufob_launch_count)
 
 #define UFOB_CUDA_TRY(expr)                                       \
     do {                                                          \

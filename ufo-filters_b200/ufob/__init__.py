@@ -105,6 +105,9 @@ def lib():
             "ufob_batch_run": ([vp, ctypes.POINTER(Job), u32, vp], i),
             "ufob_batch_destroy": ([vp], None),
             "ufob_phantom_sinogram": ([vp, u32, u32, u32, d, d, d, vp, vp], i),
+            "ufob_phantom_stack": ([vp, u32, u32, u32, u32, d, d, d, vp, vp], i),
+            "ufob_launch_count": ([], ctypes.c_uint64),
+            "ufob_measure_peaks": ([ctypes.POINTER(d), ctypes.POINTER(d)], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -437,3 +440,29 @@ def phantom_sinogram(ellipses, width, n_angles, angle_step=None, axis=None, scal
     check(lib().ufob_phantom_sinogram(ell.ctypes.data, len(ell), width, n_angles, step, axis, scale, _ptr(out),
                                       _stream(stream)))
     return out
+
+
+def phantom_stack(ellipsoids, width, n_angles, nslices, angle_step=None, axis=None, scale=None, out=None,
+                  stream=None):
+    """Analytic ellipsoid sinogram stack [nslices, n_angles, width] computed on the device."""
+    import numpy as np
+    import torch
+    ell = np.ascontiguousarray(ellipsoids, dtype=np.float64)
+    step = math.pi / n_angles if angle_step is None else angle_step
+    axis = width / 2.0 if axis is None else axis
+    scale = width / 2.0 if scale is None else scale
+    out = torch.empty((nslices, n_angles, width), dtype=torch.float32, device="cuda") if out is None else out
+    check(lib().ufob_phantom_stack(ell.ctypes.data, len(ell), width, n_angles, nslices, step, axis, scale,
+                                   _ptr(out), _stream(stream)))
+    return out
+
+
+def launch_count():
+    return int(lib().ufob_launch_count())
+
+
+def measure_peaks():
+    """(shared-memory GB/s, FP32 TFLOP/s) sustained by this device."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    check(lib().ufob_measure_peaks(ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
