@@ -1,0 +1,421 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FBP engine on the batched parallel-beam workload:
+a stack of 2048 sinograms, each 2048 detector bins x 1500 angles on [0, pi),
+filtered (fft ! filter ! ifft, ramp-fromreal) and backprojected to 2048 x 2048
+slices.  Metric: voxel-angle updates per second (GUPS), for plain FP32 and for
+FP16 filtered-sinogram storage with compensated FP32 accumulation, each with
+its relative L2 error against the FP64 oracle on a seeded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ufob|reference]
+
+One step = one pass of the engine over the whole stack (inputs resident in
+HBM).  Multi-GPU: one process per GPU (torchrun); every rank reconstructs its
+own full stack (independent slices, no collective in the data path: weak
+scaling); the step time is the max over ranks.  Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ufo-filters_b200"))
+
+METRIC = "FBP GUPS (voxel·angle updates/s), 2048²×1500, 1 B200; chosen vs plain at error"
+WORKLOAD = "batched parallel-beam FBP: 2048 slices x 2048 px x 1500 angles on [0, pi), float32"
+I0 = 1.0e4  # photons per ray (Beer-Lambert + Poisson noise)
+
+
+def parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ufob", "reference"], default="ufob")
+    ap.add_argument("--slices", type=int, default=2048)
+    ap.add_argument("--width", type=int, default=2048)
+    ap.add_argument("--angles", type=int, default=1500)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-slices", type=int, default=0, help="0 = as many as host memory allows (<= --slices)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- synthetic input
+
+def random_ellipsoids(seed, n=50, semi=(0.05, 0.4), density=(-0.5, 1.0)):
+    """50 random ellipsoids: centres uniform in the unit ball, semi-axes U[0.05, 0.4],
+    rotation about z U[0, pi), densities U[-0.5, 1]."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    v *= rng.uniform(0, 1, (n, 1)) ** (1.0 / 3.0)
+    ell = np.concatenate([v, rng.uniform(*semi, (n, 3)), rng.uniform(0, math.pi, (n, 1)),
+                          rng.uniform(*density, (n, 1))], axis=1)
+    return np.ascontiguousarray(ell, dtype=np.float64)
+
+
+def make_stack(ufob, torch, nz, P, W, seed, device, chunk=64):
+    """Noisy sinogram stack [nz, P, W] on the device: analytic ellipsoid line
+    integrals (unit-ball phantom, radius W/2 px), Beer-Lambert with I0 photons,
+    Poisson noise, -log, back to pixel-length units."""
+    ell = random_ellipsoids(seed)
+    scale = W / 2.0
+    stack = torch.empty((nz, P, W), dtype=torch.float32, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    for z0 in range(0, nz, chunk):
+        n = min(chunk, nz - z0)
+        e = ell.copy()
+        e[:, 2] -= (z0 + 0.5 * n - 0.5 * nz) / scale  # slice heights of this chunk within the stack
+        ufob.phantom_stack(e, W, P, n, out=stack[z0:z0 + n])
+        s = stack[z0:z0 + n]
+        counts = torch.poisson(I0 * torch.exp(-s / scale), generator=gen)
+        s.copy_(-torch.log(torch.clamp(counts, min=0.5) / I0) * scale)
+    torch.cuda.synchronize()
+    return stack
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], None, [], set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"],
+                                 f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "power_w_median": statistics.median(power) if power else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------- CPU leg (oracle)
+
+def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
+    """CPU baseline and FP64 error reference.  The oracle (C restatement of the
+    reference's fft ! filter ! ifft ! backproject, OpenMP on all host cores)
+    reconstructs a fixed ROI of the sampled slices in FP64; its wall time gives
+    the CPU GUPS and its output is the FP64 reference for the error report."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    rx, ry, rw, rh = roi
+    t0 = time.perf_counter()
+    refs = []
+    for s in stack_host_slices:
+        filt = oracle.fft_filter_ifft(s).astype(np.float32)
+        refs.append(oracle.backproject(filt, roi_x=rx, roi_y=ry, roi_width=rw, roi_height=rh))
+    dt = time.perf_counter() - t0
+    updates = len(stack_host_slices) * rw * rh * P
+    errors = {k: float(np.linalg.norm(np.stack(v) - np.stack(refs)) / np.linalg.norm(np.stack(refs)))
+              for k, v in gpu_rois.items()}
+    cores = os.cpu_count()
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": cores, "kind": "port",
+            "sample": "FP64 oracle FBP of a %dx%d ROI of %d slices (%d angles), %.2e updates, %.1f s"
+                      % (rw, rh, len(stack_host_slices), P, updates, dt)}, errors
+
+
+def reference_arm(args):
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores, on a bounded sample of the same workload per step."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    W, P = args.width, args.angles
+    ell = random_ellipsoids(args.seed)
+    ell2 = oracle.ellipsoid_slice_ellipses(ell, args.slices // 2, args.slices, W / 2.0)
+    sino = oracle.ellipse_sinogram(ell2, W, np.arange(P) * math.pi / P).astype(np.float32)
+    # one step = full fft ! filter ! ifft of the slice and backprojection of a centred ROI
+    side = 384
+    roi = ((W - side) // 2, (W - side) // 2, side, side)
+    kind = "port"
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        filt = oracle.fft_filter_ifft(sino).astype(np.float32)
+        oracle.backproject(filt, roi_x=roi[0], roi_y=roi[1], roi_width=side, roi_height=side)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    dt = statistics.mean(times)
+    upd = side * side * P
+    val = upd / dt / 1e9
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "GUPS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic ellipsoid phantom slice",
+            "config": {"workload": WORKLOAD, "sample_per_step": "one %dx%d slice filtered, %dx%d ROI backprojected"
+                       % (W, P, side, side)},
+            "cpu_baseline": {"value": val, "unit": "GUPS", "cores": cores, "kind": kind,
+                             "sample": "%d x %d ROI x %d angles per step (%.2e updates)" % (side, side, P, upd)},
+            "e2e": {"value": val, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's own build needs ufo-core, glib and an OpenCL runtime, absent on this box; "
+                    "this arm runs the CPU restatement of its fft ! filter ! ifft ! backproject path"}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- main arm
+
+def read_profile_traffic(name):
+    """Per-update DRAM bytes of a kernel from its committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_update:\s*([0-9.eE+-]+)", text)
+    return float(m.group(1)) if m else None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import numpy as np
+    import torch
+    import ufob
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    Z, P, W = args.slices, args.angles, args.width
+    updates_per_step = float(Z) * W * W * P
+    smem_gbs, fp32_tflops = ufob.measure_peaks()
+    stack = make_stack(ufob, torch, Z, P, W, args.seed + rank, dev)
+    vol = torch.empty((Z, W, W), dtype=torch.float32, device=dev)
+
+    # sampled slices / ROI for the FP64 error check
+    rng = np.random.default_rng(args.seed)
+    slice_ids = sorted(rng.choice(Z, size=min(4, Z), replace=False).tolist())
+    side = min(256, W)
+    if W >= 2 * side:
+        rx, ry = [int(v) for v in rng.integers(W // 4, 3 * W // 4 - side // 2, size=2)]
+    else:
+        rx = ry = 0
+    roi = (rx, ry, side, side)
+
+    gpu_id = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    forms = {}
+    launches_before = ufob.launch_count()
+    total_launches = 0
+    clocks_all = []
+    for name, storage in (("plain_fp32", ufob.F32), ("fp16_storage_kahan", ufob.F16)):
+        fbp = ufob.FBP(bp_props={"axis_pos": W / 2.0, "compensated": 0 if storage == ufob.F32 else 1},
+                       storage=storage)
+        for _ in range(args.warmup):
+            fbp.process(stack, out=vol)
+        torch.cuda.synchronize()
+        fbp.set_timing(True)
+        barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(gpu_id)
+        sampler.start()
+        l0 = ufob.launch_count()
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            fbp.process(stack, out=vol)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop()
+        clocks_all.append(clocks)
+        launches = ufob.launch_count() - l0
+        total_launches += launches
+        ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+        kt = fbp.kernel_times()
+        fbp.set_timing(False)
+        ufob.device_status()
+        gpu_rois = vol[slice_ids, ry:ry + side, rx:rx + side].double().cpu().numpy()
+        forms[name] = {"ms_per_step": ms, "gups": updates_per_step * world / (ms * 1e-3) / 1e9,
+                       "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
+                       "kernel_launches_per_step": {k: v[1] / args.steps for k, v in kt.items()},
+                       "launches_per_step": launches / args.steps, "_rois": gpu_rois, "clocks": clocks}
+        del fbp
+
+    # CPU leg: oracle timing on a bounded sample + FP64 error reference (rank 0 only)
+    cpu = None
+    if rank == 0:
+        host_slices = [stack[i].cpu().numpy() for i in slice_ids]
+        cpu, errs = cpu_leg(host_slices, slice_ids, roi, P, W, args.cpu_seconds,
+                            {k: v["_rois"] for k, v in forms.items()})
+        for k in forms:
+            forms[k]["rel_l2_vs_fp64"] = errs[k]
+    for k in forms:
+        forms[k].pop("_rois")
+
+    plain, fast = forms["plain_fp32"], forms["fp16_storage_kahan"]
+    chosen_name = "fp16_storage_kahan" if (fast.get("rel_l2_vs_fp64", 1.0) <= 1e-3 and fast["gups"] > plain["gups"]) \
+        else "plain_fp32"
+    chosen = forms[chosen_name]
+    storage = ufob.F16 if chosen_name == "fp16_storage_kahan" else ufob.F32
+
+    # end to end through the public host-pointer API (pinned host buffers, copies in the timed region)
+    e2e = None
+    if not args.no_e2e:
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = 64 << 30
+        per_slice = P * W * 4 + W * W * 4
+        nz_e2e = args.e2e_slices or min(Z, max(8, int(0.35 * avail / world / per_slice) // 8 * 8))
+        nz_e2e = min(nz_e2e, Z)
+        h_in = torch.empty((nz_e2e, P, W), dtype=torch.float32, pin_memory=True)
+        h_in.copy_(stack[:nz_e2e])
+        h_out = torch.empty((nz_e2e, W, W), dtype=torch.float32, pin_memory=True)
+        del stack
+        del vol
+        torch.cuda.empty_cache()
+        fbp = ufob.FBP(bp_props={"axis_pos": W / 2.0, "compensated": 0 if storage == ufob.F32 else 1},
+                       storage=storage)
+        fbp.process_host(h_in[:min(16, nz_e2e)], out=h_out[:min(16, nz_e2e)], slices_per_chunk=16)
+        times = []
+        for i in range(max(1, min(args.steps, 2))):
+            barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fbp.process_host(h_in, out=h_out, slices_per_chunk=64)
+            torch.cuda.synchronize()
+            times.append(max_over_ranks(time.perf_counter() - t0))
+        dt = statistics.mean(times)
+        e2e = {"value": nz_e2e * float(W) * W * P * world / dt / 1e9, "unit": "GUPS",
+               "h2d_bytes_per_step": nz_e2e * P * W * 4, "d2h_bytes_per_step": nz_e2e * W * W * 4,
+               "slices": nz_e2e, "s_per_step": dt,
+               "api": "ufob_fbp_run_host (C ABI), pinned host buffers, 64-slice chunks on two streams"}
+        del fbp, h_in, h_out
+
+    # roofline of the dominant kernel (backprojection)
+    bp_ms, bp_n = chosen["kernel_ms_per_step"]["backproject"], chosen["kernel_launches_per_step"]["backproject"]
+    gather_bytes = 8.0 if storage == ufob.F32 else 4.0  # on-chip bytes per update: 2 FP32 taps / 1 FP16 pair
+    upd_per_launch = updates_per_step / bp_n
+    avg_launch_s = bp_ms / bp_n * 1e-3
+    achieved = upd_per_launch * gather_bytes / avg_launch_s / 1e9
+    traffic_per_upd = read_profile_traffic("bp_linear_c1.md")
+    roofline = {"bound": "smem", "kernel": "k_bp_linear", "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
+                "frac": achieved / smem_gbs,
+                "traffic": traffic_per_upd * upd_per_launch if traffic_per_upd is not None else None,
+                "algorithmic_bytes_per_update": gather_bytes,
+                "peak_source": "measured on this GPU by ufob_measure_peaks (32-bit shared loads); MEASURED_PEAKS.json "
+                               "has no shared-memory figure",
+                "gups_achieved_kernel": upd_per_launch / avg_launch_s / 1e9,
+                "gups_roofline": smem_gbs / gather_bytes,
+                "fp32_tflops_measured": fp32_tflops}
+    hbm_peak = None
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except Exception:
+        pass
+    f_ms, f_n = chosen["kernel_ms_per_step"]["filter"], chosen["kernel_launches_per_step"]["filter"]
+    f_bytes = Z * P * W * 4.0 + Z * P * (W if storage == ufob.F32 else (W + 4)) * 4.0
+    roofline_filter = {"bound": "hbm", "kernel": "k_filter_rows", "achieved": f_bytes / (f_ms * 1e-3) / 1e9,
+                       "peak": hbm_peak, "unit": "GB/s",
+                       "frac": (f_bytes / (f_ms * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
+                       "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
+
+    clk = dict(chosen["clocks"])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": chosen["gups"], "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": chosen["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if storage == ufob.F32 else "f32 accumulate, f16 filtered-sinogram storage",
+            "data": "synthetic: 50 random ellipsoids, analytic line integrals, Beer-Lambert I0=1e4 + Poisson noise",
+            "config": {"workload": WORKLOAD, "slices_per_gpu": Z, "width": W, "angles": P,
+                       "chosen_form": chosen_name, "parallelism": "independent slices per GPU" if world > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (%.1f GB sinogram stack per GPU)" % (Z * P * W * 4 / 1e9),
+                       "error_sample": "slices %s, ROI x=%d y=%d %dx%d" % (slice_ids, rx, ry, side, side)},
+            "forms": forms,
+            "roofline": roofline,
+            "roofline_filter": roofline_filter,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(round(chosen["launches_per_step"] * args.steps)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

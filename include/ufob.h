@@ -176,9 +176,15 @@ ufob_status ufob_fbp_run(ufob_fbp *fbp, const float *d_sino, uint32_t width, uin
                          float *d_out, void *stream);
 ufob_status ufob_fbp_run_host(ufob_fbp *fbp, const float *h_sino, uint32_t width, uint32_t height,
                               uint32_t nslices, float *h_out, uint32_t slices_per_chunk);
-/* Output size and the backprojection kernel time of the last run, if timed. */
 ufob_status ufob_fbp_get_requisition(ufob_fbp *fbp, uint32_t width, uint32_t height, uint32_t *out_width,
                                      uint32_t *out_height);
+/* Per-kernel timing: with timing enabled every filter and backprojection
+ * launch of later runs is bracketed by CUDA events on its stream;
+ * ufob_fbp_kernel_times() synchronises on them and returns the summed
+ * durations and launch counts since timing was (re)enabled. */
+ufob_status ufob_fbp_set_timing(ufob_fbp *fbp, int enable);
+ufob_status ufob_fbp_kernel_times(ufob_fbp *fbp, double *filter_ms, uint32_t *filter_launches, double *bp_ms,
+                                  uint32_t *bp_launches);
 void ufob_fbp_destroy(ufob_fbp *fbp);
 
 /* ------------------------------------------------------ general-backproject

@@ -511,8 +511,23 @@ struct ufob_fbp {
     DevBuf hout[2];     // device staging of host output chunks
     cudaStream_t s_copy = nullptr, s_comp = nullptr;
     cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    // optional per-kernel timing: event pairs around every filter / backprojection launch
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> t_filter, t_bp;
+    size_t ev_used = 0;
+    cudaEvent_t next_event()
+    {
+        if (ev_used == ev_pool.size()) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
     ~ufob_fbp()
     {
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         ufob_filter_destroy(f);
         ufob_backproject_destroy(bp);
         for (int i = 0; i < 2; i++) {
@@ -562,10 +577,59 @@ static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, u
     const bool pairs = x->storage != UFOB_F32;
     const uint32_t pitch = pairs ? round_up(fw + 1, 4) : round_up(fw, 4);
     UFOB_TRY(x->work.ensure((size_t)pitch * 4 * height * nz));
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    if (x->timing) {
+        e0 = x->next_event();
+        e1 = x->next_event();
+        e2 = x->next_event();
+        if (!e0 || !e1 || !e2) return fail(UFOB_ERR_CUDA, "fbp: cannot create timing events");
+        UFOB_CUDA_TRY(cudaEventRecord(e0, s));
+    }
     UFOB_TRY(filter_rows_launch(x->f->plan, d_sino, width, height * nz, width, x->work.ptr, x->storage,
                                 pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw, pitch, s));
-    return ufob_backproject_run(x->bp, x->work.ptr, x->storage, pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw, height,
-                                nz, pitch, (uint64_t)pitch * height, d_out, s);
+    if (x->timing) UFOB_CUDA_TRY(cudaEventRecord(e1, s));
+    UFOB_TRY(ufob_backproject_run(x->bp, x->work.ptr, x->storage, pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw,
+                                  height, nz, pitch, (uint64_t)pitch * height, d_out, s));
+    if (x->timing) {
+        UFOB_CUDA_TRY(cudaEventRecord(e2, s));
+        x->t_filter.emplace_back(e0, e1);
+        x->t_bp.emplace_back(e1, e2);
+    }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_fbp_set_timing(ufob_fbp *x, int enable)
+{
+    if (!x) return fail(UFOB_ERR_INVALID, "fbp handle is NULL");
+    x->timing = enable != 0;
+    x->t_filter.clear();
+    x->t_bp.clear();
+    x->ev_used = 0;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_fbp_kernel_times(ufob_fbp *x, double *filter_ms, uint32_t *filter_launches, double *bp_ms,
+                                             uint32_t *bp_launches)
+{
+    if (!x) return fail(UFOB_ERR_INVALID, "fbp handle is NULL");
+    double f = 0.0, b = 0.0;
+    for (auto &p : x->t_filter) {
+        float ms = 0.f;
+        UFOB_CUDA_TRY(cudaEventSynchronize(p.second));
+        UFOB_CUDA_TRY(cudaEventElapsedTime(&ms, p.first, p.second));
+        f += ms;
+    }
+    for (auto &p : x->t_bp) {
+        float ms = 0.f;
+        UFOB_CUDA_TRY(cudaEventSynchronize(p.second));
+        UFOB_CUDA_TRY(cudaEventElapsedTime(&ms, p.first, p.second));
+        b += ms;
+    }
+    if (filter_ms) *filter_ms = f;
+    if (filter_launches) *filter_launches = (uint32_t)x->t_filter.size();
+    if (bp_ms) *bp_ms = b;
+    if (bp_launches) *bp_launches = (uint32_t)x->t_bp.size();
+    return UFOB_OK;
 }
 
 static uint32_t group_slices(uint32_t width, uint32_t height, uint32_t nslices)

@@ -91,6 +91,8 @@ def lib():
             "ufob_fbp_run_host": ([vp, vp, u32, u32, u32, vp, u32], i),
             "ufob_fbp_get_requisition": ([vp, u32, u32, pu32, pu32], i),
             "ufob_fbp_destroy": ([vp], None),
+            "ufob_fbp_set_timing": ([vp, i], i),
+            "ufob_fbp_kernel_times": ([vp, ctypes.POINTER(d), pu32, ctypes.POINTER(d), pu32], i),
             "ufob_gbp_create": ([ctypes.POINTER(vp)], i),
             "ufob_gbp_set_property": ([vp, cs, d], i),
             "ufob_gbp_set_property_string": ([vp, cs, cs], i),
@@ -327,6 +329,17 @@ class FBP:
         out = torch.empty((Z, oh, ow), dtype=torch.float32, device=s3.device) if out is None else out
         check(lib().ufob_fbp_run(self._h, _ptr(s3), W, H, Z, _ptr(out), _stream(stream)))
         return out[0] if squeeze else out
+
+    def set_timing(self, enable=True):
+        check(lib().ufob_fbp_set_timing(self._h, int(enable)))
+
+    def kernel_times(self):
+        """{'filter': (ms, launches), 'backproject': (ms, launches)} since set_timing()."""
+        fm, bm = ctypes.c_double(), ctypes.c_double()
+        fl, bl = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_fbp_kernel_times(self._h, ctypes.byref(fm), ctypes.byref(fl), ctypes.byref(bm),
+                                          ctypes.byref(bl)))
+        return {"filter": (fm.value, fl.value), "backproject": (bm.value, bl.value)}
 
     def process_host(self, sino, out=None, slices_per_chunk=32):
         """Host tensors/arrays in, host out; copies overlap compute inside the engine."""
