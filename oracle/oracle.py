@@ -331,6 +331,53 @@ def general_backproject(proj, num_projections, region=(0.0, 0.0, 0.0), x_region=
     return out
 
 
+def _to_half(x):
+    return np.asarray(x, dtype=np.float64).astype(np.float16).astype(np.float64)
+
+
+def general_backproject_store(proj, num_projections, store_type="float", gray_map_min=0.0, gray_map_max=0.0,
+                              burst=8, **kw):
+    """``general-backproject`` with the reference's store-type accumulation: the
+    generated kernel adds norm * (sum over one burst of projections) into the
+    volume in the store type once per burst (general_bp_body.in,
+    make_type_conversion :705-719): integer types clamp the gray-mapped value,
+    truncate and wrap; half rounds to half at every addition."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    n = num_projections
+    overall = kw.get("overall_angle", 2 * math.pi)
+    norm = abs(overall) / n
+    geom = dict(kw)
+    tomo = geom.pop("axis-angle-z", None)
+    if tomo is None or np.size(tomo) != n:
+        tomo = np.arange(n, dtype=np.float64) / n * overall
+    arrays = {k: v for k, v in geom.items() if k in GEOM_COLS and np.size(v) == n and n > 1}
+    acc = None
+    maxv = {"uchar": 255.0, "ushort": 65535.0, "uint": 4294967295.0}.get(store_type)
+    mod = {"uchar": 256, "ushort": 65536, "uint": 2 ** 32}.get(store_type)
+    for b0 in range(0, n, burst):
+        b1 = min(n, b0 + burst)
+        sub = dict(geom)
+        for k, v in arrays.items():
+            sub[k] = np.asarray(v)[b0:b1]
+        sub["axis-angle-z"] = np.asarray(tomo)[b0:b1]
+        sub["overall_angle"] = overall
+        part = general_backproject(proj[b0:b1], b1 - b0, **sub) / (abs(overall) / (b1 - b0))  # burst sum
+        contrib = norm * part
+        if acc is None:
+            acc = np.zeros_like(contrib)
+        if store_type == "float":
+            acc = (acc.astype(np.float32) + contrib.astype(np.float32)).astype(np.float64)
+        elif store_type == "double":
+            acc = acc + contrib
+        elif store_type == "half":
+            acc = _to_half(_to_half(acc) + _to_half(contrib))
+        else:
+            gs = maxv / (gray_map_max - gray_map_min)
+            gv = np.clip(gs * (contrib - gray_map_min), 0.0, maxv)
+            acc = np.mod(acc + np.trunc(gv), mod)
+    return acc
+
+
 def forwardproject(slice_img, n_angles, axis_pos, angle_step):
     img = np.ascontiguousarray(slice_img, dtype=np.float32)
     W = img.shape[-1]

@@ -1,0 +1,759 @@
+// General backprojection (the `general-backproject` task): parallel beam,
+// cone beam and laminography with arbitrary tilted axis, detector and volume.
+//
+// Reference: src/ufo-general-backproject-task.c.  The reference generates an
+// OpenCL kernel per geometry class (make_kernel :1069-1180) whose per-voxel
+// code is, per projection (make_transformations :909-1048):
+//   voxel_0 = (x0 + ix*dx, y0 + iy*dy, z)      (region mapping, general_bp_body.in)
+//   cone: voxel_0 *= -s.y / (d.y - s.y)        (magnification)
+//   voxel_0 = Rx(vol_x) Ry(vol_y) Rz(vol_z) voxel_0   (volume rotation)
+//   V = Rx(axis_x) Ry(axis_y) Rz(tomo_p) voxel_0     (tomographic rotation, tilted axis)
+//   project V onto the detector plane (parallel or from the source s), shift
+//   by -d, rotate by the inverse detector angles, add the centre, sample the
+//   projection bilinearly; cone beam weighs by coeff^2 = ((s.y-d.y)/(s.y-V.y))^2.
+//   volume (store-type) += norm * sum over each burst of projections.
+//
+// B200 design.  Every step before the sampling is affine in
+// X = (ix, iy, z, 1), and the cone-beam projection divides two affine forms,
+// so the whole chain of one projection is four rows of a 4x4 table:
+//   u = Nu.X / D.X,  v = Nv.X / D.X,  weight = (K / C.X)^2 (cone)  (D = C = e4, K = 1 parallel)
+// The tables are built on the device in FP64 (one thread per projection, or
+// per projection and slice when the swept parameter is not z) and cast to the
+// compute type.  The backprojection kernel gives each thread a column of ZT
+// voxels along z, so the x/y part of every dot product is formed once per
+// projection; table blocks are staged in shared memory; interpolation uses
+// exact FP32 weights with the reference's addressing modes.
+#include <cuda_fp16.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+
+#include "ufob_internal.h"
+
+namespace ufob {
+
+enum { GC_TOMO = 0, GC_AXIS_X, GC_AXIS_Y, GC_VOL_X, GC_VOL_Y, GC_VOL_Z, GC_DET_AX, GC_DET_AY, GC_DET_AZ,
+       GC_CENTER_X, GC_CENTER_Z, GC_SRC_X, GC_SRC_Y, GC_SRC_Z, GC_DET_X, GC_DET_Y, GC_DET_Z, GC_NCOLS };
+
+enum { GF_WITH_AXIS = 1, GF_WITH_VOLUME = 2, GF_PERPENDICULAR = 4, GF_SHIFTED_DETECTOR = 8, GF_SHIFTED_SOURCE = 16,
+       GF_PARALLEL = 32 };
+
+enum StoreKind { ST_HALF = 0, ST_FLOAT, ST_DOUBLE, ST_UCHAR, ST_USHORT, ST_UINT };
+enum ResultKind { RT_HALF = 0, RT_FLOAT, RT_DOUBLE };
+enum AddrKind { AD_NONE = 0, AD_CLAMP_TO_EDGE, AD_CLAMP, AD_REPEAT, AD_MIRRORED_REPEAT };
+
+static constexpr int kTab = 20;  // Nu[4] Nv[4] D[4] C[4] K pad[3]
+
+__device__ __forceinline__ float fmaf_ct(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaf_ct(double a, double b, double c) { return fma(a, b, c); }
+
+struct d3 {
+    double x, y, z;
+};
+__device__ __forceinline__ d3 rx(double s, double c, d3 p) { return {p.x, c * p.y - s * p.z, s * p.y + c * p.z}; }
+__device__ __forceinline__ d3 ry(double s, double c, d3 p) { return {c * p.x + s * p.z, p.y, -s * p.x + c * p.z}; }
+__device__ __forceinline__ d3 rz(double s, double c, d3 p) { return {c * p.x - s * p.y, s * p.x + c * p.y, p.z}; }
+
+// 4-component row vectors of affine forms in X = (ix, iy, z, 1)
+struct Row {
+    double a[4];
+};
+__device__ __forceinline__ Row rsc(Row r, double k)
+{
+    for (int i = 0; i < 4; i++) r.a[i] *= k;
+    return r;
+}
+__device__ __forceinline__ Row radd(Row p, Row q)
+{
+    for (int i = 0; i < 4; i++) p.a[i] += q.a[i];
+    return p;
+}
+__device__ __forceinline__ Row rconst(double k)
+{
+    Row r = {{0.0, 0.0, 0.0, k}};
+    return r;
+}
+struct Rows3 {
+    Row x, y, z;
+};
+// rotate a triple of rows (a linear map applied component-wise)
+__device__ __forceinline__ Rows3 rot_rows(int axis, double s, double c, Rows3 p)
+{
+    Rows3 o = p;
+    if (axis == 0) {
+        o.y = radd(rsc(p.y, c), rsc(p.z, -s));
+        o.z = radd(rsc(p.y, s), rsc(p.z, c));
+    } else if (axis == 1) {
+        o.x = radd(rsc(p.x, c), rsc(p.z, s));
+        o.z = radd(rsc(p.x, -s), rsc(p.z, c));
+    } else {
+        o.x = radd(rsc(p.x, c), rsc(p.y, -s));
+        o.y = radd(rsc(p.x, s), rsc(p.y, c));
+    }
+    return o;
+}
+
+// One table entry per (slice-or-0, projection).  geom: [n_proj][GC_NCOLS]
+// FP64; when param_col >= 0 the column is replaced by slice_values[slice].
+__global__ void k_gbp_tables(const double *__restrict__ geom, uint32_t n_proj, uint32_t n_tab_slices, int param_col,
+                             const double *__restrict__ slice_values, int flags, double x0, double dxs, double y0,
+                             double dys, float *__restrict__ tf, double *__restrict__ td)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t sl = blockIdx.y;
+    if (p >= n_proj || sl >= n_tab_slices) return;
+    double g[GC_NCOLS];
+    for (int i = 0; i < GC_NCOLS; i++) g[i] = geom[(size_t)p * GC_NCOLS + i];
+    if (param_col >= 0) g[param_col] = slice_values[sl];
+    const bool parallel = flags & GF_PARALLEL, perp = flags & GF_PERPENDICULAR;
+    const double sx = g[GC_SRC_X], sy = g[GC_SRC_Y], sz = g[GC_SRC_Z];
+    const double dx = g[GC_DET_X], dy = g[GC_DET_Y], dz = g[GC_DET_Z];
+    double s_, c_;
+
+    // columns of the affine map X -> voxel_0, pushed through the linear chain
+    d3 col[4] = {{dxs, 0.0, 0.0}, {0.0, dys, 0.0}, {0.0, 0.0, 1.0}, {x0, y0, 0.0}};
+    for (int j = 0; j < 4; j++) {
+        d3 v = col[j];
+        if (!parallel) {
+            const double m = -sy / (dy - sy);
+            v = {v.x * m, v.y * m, v.z * m};
+        }
+        if (flags & GF_WITH_VOLUME) {
+            sincos(g[GC_VOL_Z], &s_, &c_); v = rz(s_, c_, v);
+            sincos(g[GC_VOL_Y], &s_, &c_); v = ry(s_, c_, v);
+            sincos(g[GC_VOL_X], &s_, &c_); v = rx(s_, c_, v);
+        }
+        sincos(g[GC_TOMO], &s_, &c_); v = rz(s_, c_, v);
+        if (flags & GF_WITH_AXIS) {
+            sincos(g[GC_AXIS_Y], &s_, &c_); v = ry(s_, c_, v);
+            sincos(g[GC_AXIS_X], &s_, &c_); v = rx(s_, c_, v);
+        }
+        col[j] = v;
+    }
+    Rows3 M;
+    for (int j = 0; j < 4; j++) {
+        M.x.a[j] = col[j].x;
+        M.y.a[j] = col[j].y;
+        M.z.a[j] = col[j].z;
+    }
+    // detector normal and offset (make_static_transformations)
+    d3 n = {0.0, -1.0, 0.0};
+    double det_off = 0.0;
+    if (!perp) {
+        sincos(g[GC_DET_AZ], &s_, &c_); n = rz(s_, c_, n);
+        sincos(g[GC_DET_AY], &s_, &c_); n = ry(s_, c_, n);
+        sincos(g[GC_DET_AX], &s_, &c_); n = rx(s_, c_, n);
+        det_off = -(dx * n.x + dy * n.y + dz * n.z);
+    }
+    // inverse detector rotation applied after the shift: x, then y, then z with negated sines
+    auto det_rot = [&](Rows3 r) {
+        double s0, c0;
+        sincos(g[GC_DET_AX], &s0, &c0); r = rot_rows(0, -s0, c0, r);
+        sincos(g[GC_DET_AY], &s0, &c0); r = rot_rows(1, -s0, c0, r);
+        sincos(g[GC_DET_AZ], &s0, &c0); r = rot_rows(2, -s0, c0, r);
+        return r;
+    };
+    const double cx = g[GC_CENTER_X], cz = g[GC_CENTER_Z];
+    Row Nu, Nv, D = rconst(1.0), C = rconst(1.0);
+    double K = 1.0;
+    if (perp && parallel) {
+        const double dxs_ = (flags & GF_SHIFTED_DETECTOR) ? dx : 0.0, dzs_ = (flags & GF_SHIFTED_DETECTOR) ? dz : 0.0;
+        Nu = radd(M.x, rconst(cx - dxs_));
+        Nv = radd(M.z, rconst(cz - dzs_));
+    } else if (perp) {
+        const double dxs_ = (flags & GF_SHIFTED_DETECTOR) ? dx : 0.0, dzs_ = (flags & GF_SHIFTED_DETECTOR) ? dz : 0.0;
+        const double ssx = (flags & GF_SHIFTED_SOURCE) ? sx : 0.0, ssz = (flags & GF_SHIFTED_SOURCE) ? sz : 0.0;
+        const Row w = radd(M.y, rconst(-sy));  // V.y - s.y
+        Nu = radd(rsc(radd(M.x, rconst(-ssx)), dy - sy), rsc(w, sx - dxs_ + cx));
+        Nv = radd(rsc(radd(M.z, rconst(-ssz)), dy - sy), rsc(w, sz - dzs_ + cz));
+        D = w;
+        C = w;
+        K = dy - sy;
+    } else if (parallel) {
+        Rows3 P;
+        P.x = radd(M.x, rconst(-dx));
+        // V.y on the detector plane: -(V.z n.z + V.x n.x + off) / n.y
+        P.y = radd(rsc(radd(radd(rsc(M.z, n.z), rsc(M.x, n.x)), rconst(det_off)), -1.0 / n.y), rconst(-dy));
+        P.z = radd(M.z, rconst(-dz));
+        P = det_rot(P);
+        Nu = radd(P.x, rconst(cx));
+        Nv = radd(P.z, rconst(cz));
+    } else {
+        const double T = -(det_off + (sx * n.x + sy * n.y + sz * n.z));
+        Rows3 Q;
+        Q.x = radd(M.x, rconst(-sx));
+        Q.y = radd(M.y, rconst(-sy));
+        Q.z = radd(M.z, rconst(-sz));
+        const Row w = radd(radd(rsc(Q.x, n.x), rsc(Q.y, n.y)), rsc(Q.z, n.z));
+        const Rows3 RQ = det_rot(Q);
+        Rows3 sd;
+        sd.x = rconst(sx - dx);
+        sd.y = rconst(sy - dy);
+        sd.z = rconst(sz - dz);
+        sd = det_rot(sd);
+        Nu = radd(rsc(RQ.x, T), rsc(w, sd.x.a[3] + cx));
+        Nv = radd(rsc(RQ.z, T), rsc(w, sd.z.a[3] + cz));
+        D = w;
+        C = radd(rconst(sy), rsc(M.y, -1.0));  // s.y - V.y
+        K = sy - dy;
+    }
+    const size_t o = ((size_t)sl * n_proj + p) * kTab;
+    double vals[kTab] = {Nu.a[0], Nu.a[1], Nu.a[2], Nu.a[3], Nv.a[0], Nv.a[1], Nv.a[2], Nv.a[3],
+                         D.a[0],  D.a[1],  D.a[2],  D.a[3],  C.a[0],  C.a[1],  C.a[2],  C.a[3], K, 0.0, 0.0, 0.0};
+    for (int i = 0; i < kTab; i++) {
+        td[o + i] = vals[i];
+        tf[o + i] = (float)vals[i];
+    }
+}
+
+// ---------------------------------------------------------------- sampling
+
+__device__ __forceinline__ float texel(const float *__restrict__ img, int W, int H, int i, int j, int addr)
+{
+    if (addr == AD_CLAMP) {
+        if ((unsigned)i >= (unsigned)W || (unsigned)j >= (unsigned)H) return 0.f;
+    } else {
+        i = min(max(i, 0), W - 1);
+        j = min(max(j, 0), H - 1);
+    }
+    return __ldg(img + (size_t)j * W + i);
+}
+
+// OpenCL linear sampler with unnormalised coordinates: texel centres at +0.5.
+template <typename CT>
+__device__ __forceinline__ float bilinear(const float *__restrict__ img, int W, int H, CT u, CT v, int addr)
+{
+    const float uu = (float)u - 0.5f, vv = (float)v - 0.5f;
+    const float fu = floorf(uu), fv = floorf(vv);
+    const float a = uu - fu, b = vv - fv;
+    const int i = (int)fu, j = (int)fv;
+    float t00, t10, t01, t11;
+    if (i >= 0 && j >= 0 && i + 1 < W && j + 1 < H) {
+        const float *q = img + (size_t)j * W + i;
+        t00 = __ldg(q);
+        t10 = __ldg(q + 1);
+        t01 = __ldg(q + W);
+        t11 = __ldg(q + W + 1);
+    } else {
+        t00 = texel(img, W, H, i, j, addr);
+        t10 = texel(img, W, H, i + 1, j, addr);
+        t01 = texel(img, W, H, i, j + 1, addr);
+        t11 = texel(img, W, H, i + 1, j + 1, addr);
+    }
+    const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
+    return fmaf(b, bot - top, top);
+}
+
+// ---------------------------------------------------------------- accumulation semantics
+
+struct StoreParams {
+    int kind;          // StoreKind
+    double gray_min;   // gray_limit.x
+    double gray_scale; // gray_limit.y = max / (gray_max - gray_min)
+    double maxval;
+};
+
+__device__ __forceinline__ float to_half_f(float x) { return __half2float(__float2half_rn(x)); }
+
+// volume (store type) += convert(norm * burst_sum), as the generated kernel
+// does once per burst (general_bp_body.in, make_type_conversion :705-719).
+template <typename CT>
+__device__ __forceinline__ void store_accumulate(double &acc, CT contrib_norm, const StoreParams &sp)
+{
+    switch (sp.kind) {
+    case ST_FLOAT: acc = (double)((float)acc + (float)contrib_norm); break;
+    case ST_DOUBLE: acc += (double)contrib_norm; break;
+    case ST_HALF: acc = (double)to_half_f(to_half_f((float)acc) + to_half_f((float)contrib_norm)); break;
+    default: {
+        CT gv = (CT)sp.gray_scale * (contrib_norm - (CT)sp.gray_min);
+        gv = gv < (CT)0 ? (CT)0 : (gv > (CT)sp.maxval ? (CT)sp.maxval : gv);
+        const uint64_t add = (uint64_t)gv;  // C cast: truncation toward zero
+        const uint64_t mod = sp.kind == ST_UCHAR ? 0x100ull : (sp.kind == ST_USHORT ? 0x10000ull : 0x100000000ull);
+        acc = (double)(((uint64_t)acc + add) % mod);
+    }
+    }
+}
+
+__device__ __forceinline__ void store_write(void *vol, size_t idx, double acc, int kind)
+{
+    switch (kind) {
+    case ST_FLOAT: reinterpret_cast<float *>(vol)[idx] = (float)acc; break;
+    case ST_DOUBLE: reinterpret_cast<double *>(vol)[idx] = acc; break;
+    case ST_HALF: reinterpret_cast<__half *>(vol)[idx] = __float2half_rn((float)acc); break;
+    case ST_UCHAR: reinterpret_cast<uint8_t *>(vol)[idx] = (uint8_t)acc; break;
+    case ST_USHORT: reinterpret_cast<uint16_t *>(vol)[idx] = (uint16_t)acc; break;
+    default: reinterpret_cast<uint32_t *>(vol)[idx] = (uint32_t)acc; break;
+    }
+}
+
+// result-type accumulation of one sample into the burst sum
+template <int RT, typename CT>
+__device__ __forceinline__ void result_add(CT &r, CT val)
+{
+    if (RT == RT_HALF) r = (CT)to_half_f((float)r + (float)val);
+    else r += val;
+}
+
+struct GBPArgs {
+    const float *proj;  // [n][H][W]
+    uint32_t W, H, n_proj;
+    uint32_t nx, ny, nz;
+    uint32_t burst;
+    const void *tab;     // [n_tab_slices][n_proj][kTab] of CT
+    const double *zvals; // z value of each slice (parameter z) or the constant slice z
+    double norm;
+    StoreParams sp;
+    int addr;
+    void *vol;
+};
+
+template <bool CONE, typename CT, int RT, bool PARAMZ, int ZT>
+__global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
+{
+    constexpr int PB = 16;  // projections per staged table block
+    __shared__ CT s_tab[PB * kTab];
+    const int ix = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int iy = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const int z0 = blockIdx.z * ZT;
+    const CT fx = (CT)ix, fy = (CT)iy;
+    CT zv[ZT];
+#pragma unroll
+    for (int k = 0; k < ZT; k++) zv[k] = (CT)a.zvals[min(z0 + k, (int)a.nz - 1)];
+    const CT *tab = reinterpret_cast<const CT *>(a.tab) + (PARAMZ ? 0 : (size_t)z0 * a.n_proj * kTab);
+    double acc[ZT];
+    CT bsum[ZT];
+#pragma unroll
+    for (int k = 0; k < ZT; k++) {
+        acc[k] = 0.0;
+        bsum[k] = (CT)0;
+    }
+    const size_t plane = (size_t)a.W * a.H;
+    uint32_t in_burst = 0;
+    for (uint32_t p0 = 0; p0 < a.n_proj; p0 += PB) {
+        const uint32_t nb = min((uint32_t)PB, a.n_proj - p0);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < nb * kTab; i += blockDim.x) s_tab[i] = tab[(size_t)p0 * kTab + i];
+        __syncthreads();
+        for (uint32_t q = 0; q < nb; q++) {
+            const CT *t = s_tab + q * kTab;
+            const float *img = a.proj + (size_t)(p0 + q) * plane;
+            const CT u_xy = fmaf_ct(t[0], fx, fmaf_ct(t[1], fy, t[3]));
+            const CT v_xy = fmaf_ct(t[4], fx, fmaf_ct(t[5], fy, t[7]));
+            CT d_xy = (CT)1, c_xy = (CT)1;
+            if (CONE) {
+                d_xy = fmaf_ct(t[8], fx, fmaf_ct(t[9], fy, t[11]));
+                c_xy = fmaf_ct(t[12], fx, fmaf_ct(t[13], fy, t[15]));
+            }
+#pragma unroll
+            for (int k = 0; k < ZT; k++) {
+                CT u = fmaf_ct(t[2], zv[k], u_xy), v = fmaf_ct(t[6], zv[k], v_xy);
+                CT wgt = (CT)1;
+                if (CONE) {
+                    const CT inv = (CT)1 / fmaf_ct(t[10], zv[k], d_xy);
+                    u *= inv;
+                    v *= inv;
+                    const CT cc = t[16] / fmaf_ct(t[14], zv[k], c_xy);
+                    wgt = cc * cc;
+                }
+                const float val = bilinear<CT>(img, (int)a.W, (int)a.H, u, v, a.addr);
+                result_add<RT, CT>(bsum[k], CONE ? (CT)val * wgt : (CT)val);
+            }
+            if (++in_burst == a.burst || p0 + q + 1 == a.n_proj) {
+#pragma unroll
+                for (int k = 0; k < ZT; k++) {
+                    store_accumulate<CT>(acc[k], (CT)a.norm * bsum[k], a.sp);
+                    bsum[k] = (CT)0;
+                }
+                in_burst = 0;
+            }
+        }
+    }
+    if (ix >= (int)a.nx || iy >= (int)a.ny) return;
+#pragma unroll
+    for (int k = 0; k < ZT; k++) {
+        if (z0 + k >= (int)a.nz) break;
+        store_write(a.vol, ((size_t)(z0 + k) * a.ny + iy) * a.nx + ix, acc[k], a.sp.kind);
+    }
+}
+
+template <bool CONE, typename CT, int RT, bool PARAMZ>
+static ufob_status launch_gbp_t(const GBPArgs &a, cudaStream_t s)
+{
+    constexpr int ZT = PARAMZ ? 4 : 1;
+    dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + ZT - 1) / ZT);
+    k_gbp<CONE, CT, RT, PARAMZ, ZT><<<grid, 256, 0, s>>>(a);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+template <bool CONE, typename CT>
+static ufob_status launch_gbp_rt(const GBPArgs &a, int rt, bool paramz, cudaStream_t s)
+{
+    switch (rt) {
+    case RT_HALF: return paramz ? launch_gbp_t<CONE, CT, RT_HALF, true>(a, s) : launch_gbp_t<CONE, CT, RT_HALF, false>(a, s);
+    case RT_DOUBLE: return paramz ? launch_gbp_t<CONE, CT, RT_DOUBLE, true>(a, s) : launch_gbp_t<CONE, CT, RT_DOUBLE, false>(a, s);
+    default: return paramz ? launch_gbp_t<CONE, CT, RT_FLOAT, true>(a, s) : launch_gbp_t<CONE, CT, RT_FLOAT, false>(a, s);
+    }
+}
+
+}  // namespace ufob
+
+using namespace ufob;
+
+// =================================================================== task object
+
+namespace {
+
+const char *kParamNames[] = {"axis-angle-x",        "axis-angle-y",        "axis-angle-z",        "volume-angle-x",
+                             "volume-angle-y",      "volume-angle-z",      "detector-angle-x",    "detector-angle-y",
+                             "detector-angle-z",    "detector-position-x", "detector-position-y", "detector-position-z",
+                             "source-position-x",   "source-position-y",   "source-position-z",   "center-position-x",
+                             "center-position-z",   "z"};
+// geometry column of each `parameter` value (-1: z); axis-angle-z is not sweepable here
+const int kParamCol[] = {GC_AXIS_X, GC_AXIS_Y, -2,         GC_VOL_X,   GC_VOL_Y,  GC_VOL_Z,    GC_DET_AX, GC_DET_AY,  GC_DET_AZ,
+                         GC_DET_X,  GC_DET_Y,  GC_DET_Z,   GC_SRC_X,   GC_SRC_Y,  GC_SRC_Z,    GC_CENTER_X, GC_CENTER_Z, -1};
+const char *kGeomNames[GC_NCOLS] = {"axis-angle-z",     "axis-angle-x",     "axis-angle-y",      "volume-angle-x",
+                                    "volume-angle-y",   "volume-angle-z",   "detector-angle-x",  "detector-angle-y",
+                                    "detector-angle-z", "center-position-x", "center-position-z", "source-position-x",
+                                    "source-position-y", "source-position-z", "detector-position-x",
+                                    "detector-position-y", "detector-position-z"};
+const char *kStoreNames[] = {"half", "float", "double", "uchar", "ushort", "uint"};
+const char *kResultNames[] = {"half", "float", "double"};
+const char *kAddrNames[] = {"none", "clamp_to_edge", "clamp", "repeat", "mirrored_repeat"};
+
+bool name_is(const char *name, const char *canon)
+{
+    if (!name) return false;
+    for (; *name && *canon; name++, canon++) {
+        char a = *name == '_' ? '-' : *name;
+        if (a != *canon) return false;
+    }
+    return *name == 0 && *canon == 0;
+}
+
+int lookup(const char *v, const char *const *names, int n)
+{
+    for (int i = 0; i < n; i++)
+        if (v && strcmp(v, names[i]) == 0) return i;
+    return -1;
+}
+
+bool almost_zero(const std::vector<double> &v)
+{
+    for (double x : v)
+        if (!(fabs(x) < 1e-7)) return false;
+    return true;
+}
+
+}  // namespace
+
+struct ufob_gbp {
+    // properties (src/ufo-general-backproject-task.c:2087-2359)
+    uint32_t burst = 0;
+    int parameter = 17;  // z
+    double z = 0.0;
+    std::vector<double> region{0, 0, 0}, x_region{0, 0, 0}, y_region{0, 0, 0};
+    std::vector<double> geom[GC_NCOLS];
+    uint32_t num_projections = 0;
+    int compute_type = 0;  // float
+    int result_type = RT_FLOAT;
+    int store_type = ST_FLOAT;
+    double overall_angle = 2 * M_PI;
+    int addressing_mode = AD_CLAMP;
+    double gray_map_min = 0.0, gray_map_max = 0.0;
+    // device state
+    DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol;
+    uint32_t pushed = 0, pw = 0, ph = 0;
+    bool volume_ready = false;
+    ufob_gbp()
+    {
+        for (int i = 0; i < GC_NCOLS; i++) geom[i] = {0.0};
+        geom[GC_SRC_Y] = {-INFINITY};
+    }
+};
+
+static int geom_col(const char *name)
+{
+    for (int i = 0; i < GC_NCOLS; i++)
+        if (name_is(name, kGeomNames[i])) return i;
+    return -1;
+}
+
+static size_t store_size(int st)
+{
+    static const size_t sz[] = {2, 4, 8, 1, 2, 4};
+    return sz[st];
+}
+
+extern "C" ufob_status ufob_gbp_create(ufob_gbp **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "gbp_create: out is NULL");
+    *out = new ufob_gbp;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n)
+{
+    if (!g || (!values && n)) return fail(UFOB_ERR_INVALID, "gbp_set_array: NULL argument");
+    std::vector<double> v(values, values + n);
+    if (name_is(name, "region") || name_is(name, "x-region") || name_is(name, "y-region")) {
+        if (n != 3) return fail(UFOB_ERR_INVALID, "%s needs 3 values (from, to, step)", name);
+        if (name_is(name, "region")) g->region = v;
+        else if (name_is(name, "x-region")) g->x_region = v;
+        else g->y_region = v;
+        g->volume_ready = false;
+        return UFOB_OK;
+    }
+    const int c = geom_col(name);
+    if (c < 0) return fail(UFOB_ERR_INVALID, "general-backproject: no array property named '%s'", name ? name : "(null)");
+    if (!n) return fail(UFOB_ERR_INVALID, "%s needs at least one value", name);
+    g->geom[c] = v;
+    g->volume_ready = false;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double v)
+{
+    if (!g) return fail(UFOB_ERR_INVALID, "gbp handle is NULL");
+    g->volume_ready = false;
+    if (name_is(name, "burst")) {
+        if (v < 0 || v > 128) return fail(UFOB_ERR_INVALID, "burst outside [0, 128]");
+        g->burst = (uint32_t)v;
+    } else if (name_is(name, "z")) g->z = v;
+    else if (name_is(name, "num-projections")) {
+        if (v < 0 || v > 32768) return fail(UFOB_ERR_INVALID, "num-projections outside [0, 32768]");
+        g->num_projections = (uint32_t)v;
+    } else if (name_is(name, "overall-angle")) g->overall_angle = v;
+    else if (name_is(name, "gray-map-min")) g->gray_map_min = v;
+    else if (name_is(name, "gray-map-max")) g->gray_map_max = v;
+    else if (geom_col(name) >= 0) return ufob_gbp_set_array(g, name, &v, 1);
+    else return fail(UFOB_ERR_INVALID, "general-backproject: no numeric property named '%s'", name ? name : "(null)");
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value)
+{
+    if (!g) return fail(UFOB_ERR_INVALID, "gbp handle is NULL");
+    g->volume_ready = false;
+    int i;
+    if (name_is(name, "parameter")) {
+        if ((i = lookup(value, kParamNames, 18)) < 0) return fail(UFOB_ERR_INVALID, "unknown parameter '%s'", value);
+        if (kParamCol[i] == -2)
+            return fail(UFOB_ERR_UNSUPPORTED, "parameter axis-angle-z (the tomographic angle) cannot be swept");
+        g->parameter = i;
+    } else if (name_is(name, "compute-type")) {
+        if ((i = lookup(value, kResultNames + 1, 2)) < 0) return fail(UFOB_ERR_INVALID, "unknown compute-type '%s'", value);
+        g->compute_type = i;
+    } else if (name_is(name, "result-type")) {
+        if ((i = lookup(value, kResultNames, 3)) < 0) return fail(UFOB_ERR_INVALID, "unknown result-type '%s'", value);
+        g->result_type = i;
+    } else if (name_is(name, "store-type")) {
+        if ((i = lookup(value, kStoreNames, 6)) < 0) return fail(UFOB_ERR_INVALID, "unknown store-type '%s'", value);
+        g->store_type = i;
+    } else if (name_is(name, "addressing-mode")) {
+        if ((i = lookup(value, kAddrNames, 5)) < 0) return fail(UFOB_ERR_INVALID, "unknown addressing-mode '%s'", value);
+        g->addressing_mode = i;
+    } else {
+        char *end = nullptr;
+        double v = value ? strtod(value, &end) : 0.0;
+        if (!value || end == value) return fail(UFOB_ERR_INVALID, "'%s' is not a number", value ? value : "(null)");
+        return ufob_gbp_set_property(g, name, v);
+    }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_gbp_setup(ufob_gbp *g)
+{
+    if (!g) return fail(UFOB_ERR_INVALID, "gbp handle is NULL");
+    if (!g->num_projections) return fail(UFOB_ERR_SETUP, "Number of projections not set");
+    if (g->gray_map_min >= g->gray_map_max && g->store_type >= ST_UCHAR)
+        return fail(UFOB_ERR_SETUP, "Gray mapping minimum must be less then the maximum");
+    for (int c = 0; c < GC_NCOLS; c++) {
+        size_t n = g->geom[c].size();
+        if (c == GC_TOMO) continue;
+        if (n != 1 && n != g->num_projections)
+            return fail(UFOB_ERR_SETUP, "%s has %zu values; it needs 1 or num-projections (%u)", kGeomNames[c], n,
+                        g->num_projections);
+    }
+    if (g->addressing_mode == AD_REPEAT || g->addressing_mode == AD_MIRRORED_REPEAT)
+        return fail(UFOB_ERR_UNSUPPORTED, "addressing-mode %s is undefined for unnormalised coordinates",
+                    kAddrNames[g->addressing_mode]);
+    return UFOB_OK;
+}
+
+static uint32_t region_size(const std::vector<double> &r) { return (uint32_t)ceil((r[1] - r[0]) / r[2]); }
+
+extern "C" ufob_status ufob_gbp_get_requisition(ufob_gbp *g, uint32_t width, uint32_t height, uint32_t *ow,
+                                                uint32_t *oh, uint32_t *ns)
+{
+    if (!g) return fail(UFOB_ERR_INVALID, "gbp handle is NULL");
+    if (!width || !height) return fail(UFOB_ERR_REQUISITION, "empty projection %ux%u", width, height);
+    // :1495-1507: default slice size is the full detector width (both x and y)
+    const uint32_t w = g->x_region[2] == 0.0 ? width : region_size(g->x_region);
+    const uint32_t h = g->y_region[2] == 0.0 ? width : region_size(g->y_region);
+    uint32_t n = 1;
+    if (!(fabs(g->region[2]) < 1e-7)) n = (uint32_t)ceil((g->region[1] - g->region[0]) / g->region[2]);
+    if (!w || !h || !n) return fail(UFOB_ERR_REQUISITION, "empty output region");
+    if (ow) *ow = w;
+    if (oh) *oh = h;
+    if (ns) *ns = n;
+    return UFOB_OK;
+}
+
+static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uint32_t H, void *d_vol, cudaStream_t s)
+{
+    UFOB_TRY(ufob_gbp_setup(g));
+    uint32_t nx, ny, nz;
+    UFOB_TRY(ufob_gbp_get_requisition(g, W, H, &nx, &ny, &nz));
+    const uint32_t n = g->num_projections;
+    // geometry table [n][GC_NCOLS]; scalars broadcast (ufo-scarray.c:95-108); tomographic angles
+    // default to i / n * overall-angle (:1435-1446)
+    std::vector<double> table((size_t)n * GC_NCOLS);
+    for (uint32_t p = 0; p < n; p++)
+        for (int c = 0; c < GC_NCOLS; c++) {
+            const std::vector<double> &v = g->geom[c];
+            double val;
+            if (c == GC_TOMO) val = v.size() == n ? v[p] : (double)p / n * g->overall_angle;
+            else val = v.size() == 1 ? v[0] : v[p];
+            table[(size_t)p * GC_NCOLS + c] = val;
+        }
+    // geometry class (node_setup :1294-1320)
+    const int pcol = kParamCol[g->parameter];
+    const bool is_axis = pcol == GC_AXIS_X || pcol == GC_AXIS_Y;
+    const bool is_vol = pcol == GC_VOL_X || pcol == GC_VOL_Y || pcol == GC_VOL_Z;
+    const bool is_det_rot = pcol == GC_DET_AX || pcol == GC_DET_AY || pcol == GC_DET_AZ;
+    const bool is_det_pos = pcol == GC_DET_X || pcol == GC_DET_Y || pcol == GC_DET_Z;
+    int flags = 0;
+    if (is_axis || !(almost_zero(g->geom[GC_AXIS_X]) && almost_zero(g->geom[GC_AXIS_Y]))) flags |= GF_WITH_AXIS;
+    if (is_vol || !(almost_zero(g->geom[GC_VOL_X]) && almost_zero(g->geom[GC_VOL_Y]) && almost_zero(g->geom[GC_VOL_Z])))
+        flags |= GF_WITH_VOLUME;
+    if (!(almost_zero(g->geom[GC_DET_X]) && almost_zero(g->geom[GC_DET_Z]))) flags |= GF_SHIFTED_DETECTOR;
+    if (!(almost_zero(g->geom[GC_SRC_X]) && almost_zero(g->geom[GC_SRC_Z]))) flags |= GF_SHIFTED_SOURCE;
+    if (!is_det_rot && !is_det_pos && almost_zero(g->geom[GC_DET_AX]) && almost_zero(g->geom[GC_DET_AY]) &&
+        almost_zero(g->geom[GC_DET_AZ]))
+        flags |= GF_PERPENDICULAR;
+    bool parallel = true;
+    for (uint32_t p = 0; p < n; p++) parallel = parallel && std::isinf(table[(size_t)p * GC_NCOLS + GC_SRC_Y]);
+    if (parallel) flags |= GF_PARALLEL;
+    // regions (compute_slice_region :280-291)
+    auto reg = [](const std::vector<double> &r, uint32_t len, double *start, double *step) {
+        if (r[2] != 0.0) {
+            *start = r[0];
+            *step = r[2];
+        } else {
+            *start = -((double)(float)len / 2.0);
+            *step = 1.0;
+        }
+    };
+    double x0, dxs, y0, dys;
+    reg(g->x_region, nx, &x0, &dxs);
+    reg(g->y_region, ny, &y0, &dys);
+    double rs = 0.0, rstep = 1.0;
+    if (!(fabs(g->region[2]) < 1e-7)) {
+        rs = g->region[0];
+        rstep = g->region[2];
+    }
+    std::vector<double> slice_values(nz);
+    for (uint32_t k = 0; k < nz; k++) slice_values[k] = rs + k * rstep;
+    const bool paramz = pcol == -1;
+    std::vector<double> zvals(nz, g->z);
+    if (paramz) zvals = slice_values;
+    const uint32_t tab_slices = paramz ? 1 : nz;
+    UFOB_TRY(g->d_geom.ensure(table.size() * sizeof(double) + nz * sizeof(double)));
+    UFOB_TRY(g->d_zvals.ensure(nz * sizeof(double) * 2));
+    UFOB_TRY(g->d_tab_f.ensure((size_t)tab_slices * n * kTab * sizeof(float)));
+    UFOB_TRY(g->d_tab_d.ensure((size_t)tab_slices * n * kTab * sizeof(double)));
+    double *d_table = g->d_geom.as<double>(), *d_slicev = d_table + table.size();
+    UFOB_CUDA_TRY(cudaMemcpyAsync(d_table, table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(d_slicev, slice_values.data(), nz * sizeof(double), cudaMemcpyHostToDevice, s));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(g->d_zvals.ptr, zvals.data(), nz * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_gbp_tables<<<dim3((n + 127) / 128, tab_slices), 128, 0, s>>>(d_table, n, tab_slices, paramz ? -1 : pcol, d_slicev,
+                                                                  flags, x0, dxs, y0, dys, g->d_tab_f.as<float>(),
+                                                                  g->d_tab_d.as<double>());
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+
+    GBPArgs a;
+    a.proj = d_proj;
+    a.W = W;
+    a.H = H;
+    a.n_proj = n;
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.burst = g->burst ? g->burst : 8;  // "GENERIC" entry of the node table (ufo-conebeam.c:21-26)
+    a.zvals = g->d_zvals.as<double>();
+    a.norm = fabs(g->overall_angle) / n;  // :292
+    a.sp.kind = g->store_type;
+    a.sp.gray_min = g->gray_map_min;
+    const double maxv = g->store_type == ST_UCHAR ? 255.0 : g->store_type == ST_USHORT ? 65535.0 : 4294967295.0;
+    a.sp.maxval = maxv;
+    a.sp.gray_scale = g->store_type >= ST_UCHAR ? maxv / (g->gray_map_max - g->gray_map_min) : 0.0;
+    a.addr = g->addressing_mode == AD_CLAMP ? AD_CLAMP : AD_CLAMP_TO_EDGE;  // "none": defined as clamp-to-edge
+    a.vol = d_vol;
+    const bool cone = !parallel;
+    if (g->compute_type == 1) {
+        a.tab = g->d_tab_d.ptr;
+        return cone ? launch_gbp_rt<true, double>(a, g->result_type, paramz, s)
+                    : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
+    }
+    a.tab = g->d_tab_f.ptr;
+    return cone ? launch_gbp_rt<true, float>(a, g->result_type, paramz, s)
+                : launch_gbp_rt<false, float>(a, g->result_type, paramz, s);
+}
+
+extern "C" ufob_status ufob_gbp_run(ufob_gbp *g, const float *d_proj, uint32_t W, uint32_t H, void *d_vol,
+                                    void *stream)
+{
+    if (!g || !d_proj || !d_vol) return fail(UFOB_ERR_INVALID, "gbp_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    return gbp_compute(g, d_proj, W, H, d_vol, (cudaStream_t)stream);
+}
+
+extern "C" ufob_status ufob_gbp_process(ufob_gbp *g, const float *d_projection, uint32_t W, uint32_t H, void *stream)
+{
+    if (!g || !d_projection) return fail(UFOB_ERR_INVALID, "gbp_process: NULL argument");
+    UFOB_TRY(ensure_device());
+    UFOB_TRY(ufob_gbp_setup(g));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (g->pushed == 0) {
+        g->pw = W;
+        g->ph = H;
+        UFOB_TRY(g->d_proj.ensure((size_t)g->num_projections * W * H * sizeof(float)));
+    }
+    if (W != g->pw || H != g->ph) return fail(UFOB_ERR_INVALID, "projection size changed within the stream");
+    if (g->pushed >= g->num_projections)
+        return fail(UFOB_ERR_INVALID, "received more than num-projections (%u) projections", g->num_projections);
+    UFOB_CUDA_TRY(cudaMemcpyAsync(g->d_proj.as<float>() + (size_t)g->pushed * W * H, d_projection,
+                                  (size_t)W * H * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    g->pushed++;
+    if (g->pushed == g->num_projections) {
+        uint32_t nx, ny, nz;
+        UFOB_TRY(ufob_gbp_get_requisition(g, W, H, &nx, &ny, &nz));
+        UFOB_TRY(g->d_vol.ensure((size_t)nx * ny * nz * store_size(g->store_type)));
+        UFOB_TRY(gbp_compute(g, g->d_proj.as<float>(), W, H, g->d_vol.ptr, s));
+        g->volume_ready = true;
+    }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_gbp_generate(ufob_gbp *g, void *d_slice, uint32_t index, void *stream)
+{
+    if (!g || !d_slice) return fail(UFOB_ERR_INVALID, "gbp_generate: NULL argument");
+    if (g->pushed != g->num_projections || !g->volume_ready)
+        return fail(UFOB_ERR_INVALID,
+                    "general-backproject received only %u projections out of %u specified, no output will be generated",
+                    g->pushed, g->num_projections);
+    uint32_t nx, ny, nz;
+    UFOB_TRY(ufob_gbp_get_requisition(g, g->pw, g->ph, &nx, &ny, &nz));
+    if (index >= nz) return fail(UFOB_ERR_INVALID, "slice %u of %u", index, nz);
+    const size_t bytes = (size_t)nx * ny * store_size(g->store_type);
+    UFOB_CUDA_TRY(cudaMemcpyAsync(d_slice, g->d_vol.as<char>() + bytes * index, bytes, cudaMemcpyDeviceToDevice,
+                                  (cudaStream_t)stream));
+    return UFOB_OK;
+}
+
+extern "C" void ufob_gbp_destroy(ufob_gbp *g) { delete g; }
