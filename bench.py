@@ -152,12 +152,19 @@ def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
+    import reference
     rx, ry, rw, rh = roi
-    t0 = time.perf_counter()
     refs = []
-    for s in stack_host_slices:
+    for s in stack_host_slices:  # FP64 oracle: the error reference
         filt = oracle.fft_filter_ifft(s).astype(np.float32)
         refs.append(oracle.backproject(filt, roi_x=rx, roi_y=ry, roi_width=rw, roi_height=rh))
+    # timed: the reference's own filter/backproject code on the host cores where its CPU build
+    # is present, else the oracle
+    impl = reference if reference.available() else oracle
+    t0 = time.perf_counter()
+    for s in stack_host_slices:
+        filt = impl.fft_filter_ifft(s).astype(np.float32)
+        impl.backproject(filt, roi_x=rx, roi_y=ry, roi_width=rw, roi_height=rh)
     dt = time.perf_counter() - t0
     updates = len(stack_host_slices) * rw * rh * P
     errors = {k: float(np.linalg.norm(np.stack(v) - np.stack(refs)) / np.linalg.norm(np.stack(refs)))
@@ -167,9 +174,12 @@ def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
         cores = len(os.sched_getaffinity(0))
     except AttributeError:
         pass
-    return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": cores, "kind": "port",
-            "sample": "FP64 oracle FBP of a %dx%d ROI of %d slices (%d angles), %.2e updates, %.1f s"
-                      % (rw, rh, len(stack_host_slices), P, updates, dt)}, errors
+    kind = "reference" if impl is reference else "port"
+    what = ("reference filter/backproject tasks and kernels compiled for the CPU (OpenMP)" if kind == "reference"
+            else "FP64 oracle")
+    return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": cores, "kind": kind,
+            "sample": "%s: fft/filter/ifft of %d full slices + backprojection of a %dx%d ROI (%d angles), "
+                      "%.2e updates, %.1f s" % (what, len(stack_host_slices), rw, rh, P, updates, dt)}, errors
 
 
 def reference_arm(args):
@@ -178,6 +188,7 @@ def reference_arm(args):
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    import reference
     if int(os.environ.get("RANK", "0")) != 0:
         return
     W, P = args.width, args.angles
@@ -187,12 +198,13 @@ def reference_arm(args):
     # one step = full fft ! filter ! ifft of the slice and backprojection of a centred ROI
     side = 384
     roi = ((W - side) // 2, (W - side) // 2, side, side)
-    kind = "port"
+    impl = reference if reference.available() else oracle
+    kind = "reference" if impl is reference else "port"
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        filt = oracle.fft_filter_ifft(sino).astype(np.float32)
-        oracle.backproject(filt, roi_x=roi[0], roi_y=roi[1], roi_width=side, roi_height=side)
+        filt = impl.fft_filter_ifft(sino).astype(np.float32)
+        impl.backproject(filt, roi_x=roi[0], roi_y=roi[1], roi_width=side, roi_height=side)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
     dt = statistics.mean(times)
@@ -201,14 +213,18 @@ def reference_arm(args):
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "GUPS", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic ellipsoid phantom slice",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if kind == "reference" else "f64",
+            "data": "synthetic: slice of the 50-ellipsoid phantom, analytic line integrals",
             "config": {"workload": WORKLOAD, "sample_per_step": "one %dx%d slice filtered, %dx%d ROI backprojected"
                        % (W, P, side, side)},
             "cpu_baseline": {"value": val, "unit": "GUPS", "cores": cores, "kind": kind,
                              "sample": "%d x %d ROI x %d angles per step (%.2e updates)" % (side, side, P, upd)},
             "e2e": {"value": val, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference's own build needs ufo-core, glib and an OpenCL runtime, absent on this box; "
-                    "this arm runs the CPU restatement of its fft ! filter ! ifft ! backproject path"}
+            "note": ("the reference's filter and backproject task sources and OpenCL kernels compiled for the "
+                     "host CPU through GLib/OpenCL/ufo-core shims (OpenMP over work-items, FP64 FFT in place of "
+                     "oclfft); ufo-core and an OpenCL CPU runtime are absent on this box"
+                     if kind == "reference" else
+                     "FP64 CPU restatement of the reference path (the reference's CPU build is absent)")}
     print(json.dumps(line), flush=True)
 
 

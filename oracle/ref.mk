@@ -9,7 +9,7 @@ GEN := $(OUT)/gen
 CC := gcc
 CXX := g++
 CFLAGS := -O2 -fopenmp -fPIC -w -Irefshim -I$(REF)/src -I$(REF)/src/common
-CXXFLAGS := -O2 -fopenmp -fPIC -std=c++17 -w -Irefshim -I$(REF)/src -I$(GEN)
+CXXFLAGS := -O2 -fopenmp -fPIC -std=c++17 -w -mfma -ffp-contract=fast -Irefshim -I$(REF)/src -I$(GEN)
 KERNELS := backproject filter fft forwardproject
 
 all: $(OUT)/libufo_ref.so

@@ -1,0 +1,62 @@
+"""Generate the golden fixtures in this folder from the reference itself.
+
+The reference's `filter` and `backproject` task sources and its OpenCL kernels
+are compiled for the CPU by oracle/ref.mk (oracle/_ref/libufo_ref.so, see
+oracle/reference.py); this script runs them on seeded inputs and stores inputs
+and outputs.  Run it where the reference sources are present:
+
+    make -C oracle -f ref.mk && python tests/golden/make_golden.py
+"""
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import oracle  # noqa: E402  (phantom generators only)
+import reference  # noqa: E402
+
+FILTER_CASES = [
+    dict(filter="ramp-fromreal"), dict(filter="ramp"), dict(filter="butterworth", cutoff=0.3, order=6.0),
+    dict(filter="faris-byer", tau=0.2, theta=0.7), dict(filter="hamming", cutoff=0.4), dict(filter="bh3"),
+    dict(filter="ramp-fromreal", scale=1.7), dict(filter="butterworth", scale=0.5),
+]
+CHAIN_CASES = [dict(), dict(size_x=128, crop_width=100), dict(size_x=128), dict(filter="hamming", cutoff=0.4),
+               dict(filter="ramp")]
+BP_CASES = [dict(), dict(axis_pos=31.5), dict(axis_pos=30.25, angle_step=0.05, angle_offset=0.3),
+            dict(roi_x=10, roi_y=5, roi_width=40, roi_height=30), dict(num_projections=80, offset=20),
+            dict(mode="nearest", roi_x=3, roi_width=50, roi_height=50)]
+
+
+def main():
+    out = {}
+    for i, c in enumerate(FILTER_CASES):
+        for n in (8, 64, 256):
+            out["coeff_%d_%d" % (i, n)] = reference.filter_coefficients(n, **c)
+    rng = np.random.default_rng(1234)
+    sino = rng.standard_normal((17, 64)).astype(np.float32)
+    out["chain_input"] = sino
+    for i, c in enumerate(CHAIN_CASES):
+        out["chain_%d" % i] = reference.fft_filter_ifft(sino, **c)
+    bp_in = rng.standard_normal((45, 64)).astype(np.float32)
+    out["bp_input"] = bp_in
+    for i, c in enumerate(BP_CASES):
+        out["bp_%d" % i] = reference.backproject(bp_in, **c)
+    # FBP of an analytic ellipse phantom, 128 px, 128 angles (the C0 recipe at a quarter size)
+    ell = oracle.random_ellipses(7)
+    W = P = 128
+    fsino = oracle.ellipse_sinogram(ell, W, np.arange(P) * math.pi / P).astype(np.float32)
+    out["fbp_input"] = fsino
+    out["fbp_output"] = reference.fbp(fsino, axis_pos=63.5)
+    img = oracle.ellipse_image(ell, 64).astype(np.float32)
+    out["fp_input"] = img
+    out["fp_output"] = reference.forwardproject(img, 30, 32.0, math.pi / 30)
+    path = os.path.join(HERE, "reference_fbp.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()
