@@ -184,15 +184,49 @@ struct BPShape {
     static constexpr size_t kSmem = kBarOffset + (size_t)S * 8 + 128;  // +128: manual base alignment
 };
 
+// Interpolation weights (1 - w, w) with w = d + 0.5 as a packed 16-bit pair
+// (lower half = weight of the lower tap): one pack and one packed FMA,
+// (d, d) * (-1, 1) + (0.5, 0.5).
 template <int KIND>
-__device__ __forceinline__ float2 unpack_pair(uint32_t v)
+__device__ __forceinline__ uint32_t pair_weights(float d)
 {
-    if (KIND == SINO_F16_PAIRS) {
-        __half2 h = *reinterpret_cast<__half2 *>(&v);
-        return __half22float2(h);
-    } else {
-        return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u));
-    }
+    uint32_t r;
+    if (KIND == SINO_F16_PAIRS)
+        asm("{\n\t.reg .b32 dd;\n\tcvt.rn.f16x2.f32 dd, %1, %1;\n\tfma.rn.f16x2 %0, dd, %2, %3;\n\t}"
+            : "=r"(r)
+            : "f"(d), "r"(0x3C00BC00u), "r"(0x38003800u));
+    else
+        asm("{\n\t.reg .b32 dd;\n\tcvt.rn.bf16x2.f32 dd, %1, %1;\n\tfma.rn.bf16x2 %0, dd, %2, %3;\n\t}"
+            : "=r"(r)
+            : "f"(d), "r"(0x3F80BF80u), "r"(0x3F003F00u));
+    return r;
+}
+
+// (a0, a1) += k * (x0, x1) as one packed FP32 FMA (sm_100 fma.rn.f32x2).
+__device__ __forceinline__ void fma2(float &a0, float &a1, float k, float x0, float x1)
+{
+    asm("{\n\t.reg .b64 a, x, kk;\n\tmov.b64 a, {%0, %1};\n\tmov.b64 x, {%2, %3};\n\tmov.b64 kk, {%4, %4};\n\t"
+        "fma.rn.f32x2 a, kk, x, a;\n\tmov.b64 {%0, %1}, a;\n\t}"
+        : "+f"(a0), "+f"(a1)
+        : "f"(x0), "f"(x1), "f"(k));
+}
+
+// acc += w_lo * s_lo + w_hi * s_hi with 16-bit operands and FP32 accumulation
+// (sm_100 mixed-precision fma.rn.f32.{f16,bf16}; the products are exact in FP32).
+template <int KIND>
+__device__ __forceinline__ float pair_fma(uint32_t pair, uint32_t wts, float acc)
+{
+    if (KIND == SINO_F16_PAIRS)
+        asm("{\n\t.reg .b16 l, h, wl, wh;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {wl, wh}, %2;\n\t"
+            "fma.rn.f32.f16 %0, wl, l, %0;\n\tfma.rn.f32.f16 %0, wh, h, %0;\n\t}"
+            : "+f"(acc)
+            : "r"(pair), "r"(wts));
+    else
+        asm("{\n\t.reg .b16 l, h, wl, wh;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {wl, wh}, %2;\n\t"
+            "fma.rn.f32.bf16 %0, wl, l, %0;\n\tfma.rn.f32.bf16 %0, wh, h, %0;\n\t}"
+            : "+f"(acc)
+            : "r"(pair), "r"(wts));
+    return acc;
 }
 
 template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
@@ -294,21 +328,37 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
                     const float vv = fmaf(by[j], sc.x, t);  // element coordinate - 0.5
                     const float r = vv + kMagic;
                     const float fe = r - kMagic;            // rint(vv) == floor(vv + 0.5)
-                    const float d = vv - fe;
-                    const float w = d + 0.5f, omw = 0.5f - d;
+                    const float d = vv - fe;                // weight of the upper tap is d + 0.5
                     uint32_t e = (uint32_t)(__float_as_int(r) - kMagicBits);
-                    e = min(e, (uint32_t)(WIN - 2));  // guard: never leaves the angle's window
+                    if (PAIRS) {
+                        // one 32-bit pair (s[j-1], s[j]) per update, FP32 accumulation of
+                        // half-precision products: no conversions in the slice loop
+                        const uint32_t wts = pair_weights<KIND>(d);
+                        e = min(e, (uint32_t)(WIN - 1));  // guard: never leaves the angle's window
 #pragma unroll
-                    for (int z = 0; z < ZT; z++) {
-                        if (PAIRS) {
-                            const float2 v = unpack_pair<KIND>(row[z * WIN + e]);
-                            part[j][z] = fmaf(omw, v.x, part[j][z]);
-                            part[j][z] = fmaf(w, v.y, part[j][z]);
+                        for (int z = 0; z < ZT; z++) part[j][z] = pair_fma<KIND>(row[z * WIN + e], wts, part[j][z]);
+                    } else {
+                        const float w = d + 0.5f, omw = 0.5f - d;
+                        e = min(e, (uint32_t)(WIN - 2));
+                        if (ZT % 2 == 0) {
+                            // two slices per packed FP32 FMA (bit-identical to two fmaf)
+#pragma unroll
+                            for (int z = 0; z < ZT; z += 2) {
+                                const float lo0 = __uint_as_float(row[z * WIN + e]);
+                                const float hi0 = __uint_as_float(row[z * WIN + e + 1]);
+                                const float lo1 = __uint_as_float(row[(z + 1) * WIN + e]);
+                                const float hi1 = __uint_as_float(row[(z + 1) * WIN + e + 1]);
+                                fma2(part[j][z], part[j][z + 1], omw, lo0, lo1);
+                                fma2(part[j][z], part[j][z + 1], w, hi0, hi1);
+                            }
                         } else {
-                            const float lo = __uint_as_float(row[z * WIN + e]);
-                            const float hi = __uint_as_float(row[z * WIN + e + 1]);
-                            part[j][z] = fmaf(omw, lo, part[j][z]);
-                            part[j][z] = fmaf(w, hi, part[j][z]);
+#pragma unroll
+                            for (int z = 0; z < ZT; z++) {
+                                const float lo = __uint_as_float(row[z * WIN + e]);
+                                const float hi = __uint_as_float(row[z * WIN + e + 1]);
+                                part[j][z] = fmaf(omw, lo, part[j][z]);
+                                part[j][z] = fmaf(w, hi, part[j][z]);
+                            }
                         }
                     }
                 }
@@ -445,6 +495,9 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
     case 2: return launch_linear<32, 32, 4, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 3: return launch_linear<32, 16, 4, 16, 4, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 4: return launch_linear<32, 32, 8, 8, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 5: return launch_linear<32, 16, 8, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 6: return launch_linear<32, 32, 8, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 7: return launch_linear<32, 16, 4, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     default: return fail(UFOB_ERR_INVALID, "backproject: unknown tile id %d", tile);
     }
 }

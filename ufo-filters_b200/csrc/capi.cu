@@ -509,7 +509,7 @@ struct ufob_fbp {
     DevBuf work;        // filtered sinograms of one slice group
     DevBuf hin[2];      // device staging of host input chunks
     DevBuf hout[2];     // device staging of host output chunks
-    cudaStream_t s_copy = nullptr, s_comp = nullptr;
+    cudaStream_t s_copy = nullptr, s_comp = nullptr, s_d2h = nullptr;  // uploads, compute, downloads
     cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
     // optional per-kernel timing: event pairs around every filter / backprojection launch
     bool timing = false;
@@ -536,6 +536,7 @@ struct ufob_fbp {
             if (ev_out[i]) cudaEventDestroy(ev_out[i]);
         }
         if (s_copy) cudaStreamDestroy(s_copy);
+        if (s_d2h) cudaStreamDestroy(s_d2h);
         if (s_comp) cudaStreamDestroy(s_comp);
     }
 };
@@ -668,6 +669,7 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
     chunk = std::min(chunk, nslices);
     if (!x->s_copy) {
         UFOB_CUDA_TRY(cudaStreamCreateWithFlags(&x->s_copy, cudaStreamNonBlocking));
+        UFOB_CUDA_TRY(cudaStreamCreateWithFlags(&x->s_d2h, cudaStreamNonBlocking));
         UFOB_CUDA_TRY(cudaStreamCreateWithFlags(&x->s_comp, cudaStreamNonBlocking));
         for (int i = 0; i < 2; i++) {
             UFOB_CUDA_TRY(cudaEventCreateWithFlags(&x->ev_in[i], cudaEventDisableTiming));
@@ -680,8 +682,8 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
         UFOB_TRY(x->hin[i].ensure(in_bytes));
         UFOB_TRY(x->hout[i].ensure(out_bytes));
     }
-    // Pipeline: H2D(c) on the copy stream -> filter+BP(c) on the compute stream -> D2H(c) on the copy stream,
-    // double-buffered so chunk c+1's upload and chunk c-1's download overlap chunk c's compute.
+    // Pipeline: H2D(c) on the upload stream -> filter+BP(c) on the compute stream -> D2H(c) on the download
+    // stream, double-buffered so chunk c+1's upload and chunk c-1's download overlap chunk c's compute.
     uint32_t c = 0;
     for (uint32_t z = 0; z < nslices; z += chunk, c++) {
         const int b = c & 1;
@@ -694,13 +696,14 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
         if (c >= 2) UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_comp, x->ev_out[b], 0));  // hout[b] downloaded
         UFOB_TRY(fbp_group(x, x->hin[b].as<float>(), width, height, nz, x->hout[b].as<float>(), x->s_comp));
         UFOB_CUDA_TRY(cudaEventRecord(x->ev_done[b], x->s_comp));
-        UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_copy, x->ev_done[b], 0));
+        UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_d2h, x->ev_done[b], 0));
         UFOB_CUDA_TRY(cudaMemcpyAsync(h_out + (size_t)z * ow * oh, x->hout[b].ptr, (size_t)nz * ow * oh * 4,
-                                      cudaMemcpyDeviceToHost, x->s_copy));
-        UFOB_CUDA_TRY(cudaEventRecord(x->ev_out[b], x->s_copy));
+                                      cudaMemcpyDeviceToHost, x->s_d2h));
+        UFOB_CUDA_TRY(cudaEventRecord(x->ev_out[b], x->s_d2h));
     }
     UFOB_CUDA_TRY(cudaStreamSynchronize(x->s_copy));
     UFOB_CUDA_TRY(cudaStreamSynchronize(x->s_comp));
+    UFOB_CUDA_TRY(cudaStreamSynchronize(x->s_d2h));
     return check_device_error_word(x->s_comp);
 }
 
