@@ -230,9 +230,20 @@ typedef struct {
     double angle_offset;
 } ufob_job;
 
+/* Each job runs `fft size-x=N ! filter ! ifft crop-width=width ! backproject`
+ * with N = fprops->size_x if set, else the next power of two >= width (the
+ * filter needs a power-of-two spectrum), and a width x width output.  Rows
+ * must be 16-byte aligned (width a multiple of 4).  The first run of a batch
+ * autotunes the backprojection tile shape (cached on disk under
+ * $UFOB_TUNE_CACHE or $HOME/.cache/ufob/tune.txt; UFOB_TUNE=0 skips tuning)
+ * and captures the batch into a CUDA graph, replayed while the jobs' pointers,
+ * sizes and geometry stay the same.  Engine addition: the reference runs one
+ * task graph per item. */
 typedef struct ufob_batch ufob_batch;
 ufob_status ufob_batch_create(const ufob_filter_props *fprops, ufob_dtype storage, ufob_batch **out);
 ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint32_t n, void *stream);
+/* Tile-shape variant the autotuner chose for the current batch (-1 before the first run). */
+int ufob_batch_variant(ufob_batch *b);
 void ufob_batch_destroy(ufob_batch *b);
 
 /* ------------------------------------------------------------- utilities */
@@ -249,6 +260,17 @@ ufob_status ufob_phantom_sinogram(const double *h_ellipses, uint32_t n_ellipses,
 ufob_status ufob_phantom_stack(const double *h_ellipsoids, uint32_t n, uint32_t width, uint32_t n_angles,
                                uint32_t nslices, double angle_step, double axis, double scale, float *d_sino,
                                void *stream);
+/* Parallel-beam forward projection of a width x width slice into
+ * [n_angles][width] by unit-step ray marching with linear sampling; replaces
+ * src/kernels/forwardproject.cl:24-58 (src/ufo-forwardproject-task.c). */
+ufob_status ufob_forwardproject(const float *d_slice, uint32_t width, uint32_t n_angles, double axis_pos,
+                                double angle_step, float *d_sino, void *stream);
+/* Rasterise ellipse phantoms into [n_images][N][N]: image i uses rows
+ * h_offsets[i] .. h_offsets[i+1]-1 of h_ellipses (cx, cy, a, b, phi, rho), pixel
+ * centres mapped to ((x + 0.5 - axis) / scale, (y + 0.5 - axis) / scale),
+ * supersample^2 samples per pixel. */
+ufob_status ufob_phantom_images(const double *h_ellipses, const uint32_t *h_offsets, uint32_t n_images, uint32_t N,
+                                double axis, double scale, int supersample, float *d_out, void *stream);
 /* Number of engine kernels launched by this process so far. */
 uint64_t ufob_launch_count(void);
 /* Sustained shared-memory load bandwidth (GB/s, 32-bit conflict-free loads)

@@ -448,3 +448,44 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# --------------------------------------------------------------------------- CNN (sparse-view correction)
+
+def conv3x3_nhwc(x, w, bias=None, relu=False):
+    """FP64 3x3 convolution, zero padding: x [N,H,W,Cin], w [Cout,9,Cin] with tap
+    t = 3*(dy+1) + (dx+1) -> [N,H,W,Cout]."""
+    x = np.asarray(x, dtype=np.float64)
+    w = np.asarray(w, dtype=np.float64)
+    N, H, W, C = x.shape
+    xp = np.zeros((N, H + 2, W + 2, C))
+    xp[:, 1:-1, 1:-1] = x
+    out = np.zeros((N, H, W, w.shape[0]))
+    for t in range(9):
+        dy, dx = t // 3 - 1, t % 3 - 1
+        out += np.einsum("nhwc,oc->nhwo", xp[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W], w[:, t])
+    if bias is not None:
+        out += np.asarray(bias, dtype=np.float64)
+    if relu:
+        out = np.maximum(out, 0.0)
+    return out
+
+
+def conv3x3_wgrad_nhwc(x, dz):
+    """dW[co][t][ci] = sum_p dz[p][co] * x[p + off(t)][ci] (FP64)."""
+    x = np.asarray(x, dtype=np.float64)
+    dz = np.asarray(dz, dtype=np.float64)
+    N, H, W, C = x.shape
+    xp = np.zeros((N, H + 2, W + 2, C))
+    xp[:, 1:-1, 1:-1] = x
+    dw = np.zeros((dz.shape[-1], 9, C))
+    for t in range(9):
+        dy, dx = t // 3 - 1, t % 3 - 1
+        dw[:, t] = np.einsum("nhwo,nhwc->oc", dz, xp[:, 1 + dy:1 + dy + H, 1 + dx:1 + dx + W])
+    return dw
+
+
+def conv3x3_dgrad_weights(w):
+    """Weights of the data-gradient convolution: [Cin][9][Cout], taps flipped."""
+    w = np.asarray(w)
+    return np.ascontiguousarray(w[:, ::-1, :].transpose(2, 1, 0))

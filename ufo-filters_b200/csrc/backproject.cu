@@ -115,7 +115,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 // 3-D map over [nz][P][elems] 4-byte elements; box = (box_x, 1, box_z).
-static ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, uint32_t P, uint32_t nz,
+ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, uint32_t P, uint32_t nz,
                                  uint32_t pitch, uint64_t slice_pitch, uint32_t box_x, uint32_t box_z)
 {
     auto fn = encode_fn();
@@ -155,15 +155,6 @@ ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_o
 }
 
 // ------------------------------------------------------------------ linear kernel
-
-struct BPArgs {
-    uint32_t P, nz;
-    uint32_t roi_x, roi_y, roi_w, roi_h;
-    float axis, norm;
-    const float2 *sincos;
-    float *out;
-    int *err;
-};
 
 template <int TX, int TY, int ZT, int A, int S>
 struct BPShape {
@@ -229,8 +220,29 @@ __device__ __forceinline__ float pair_fma(uint32_t pair, uint32_t wts, float acc
     return acc;
 }
 
+// Shared-memory carve-up of one backprojection CTA.
+template <typename Sh>
+struct BPSmem {
+    uint32_t *data;  // [S][A][ASTR], angle box = [ZT][WIN]
+    int *win;        // [S][A] TMA x origin of each staged window
+    uint64_t *full;  // [S] mbarriers
+    __device__ __forceinline__ explicit BPSmem(unsigned char *smem_dyn)
+    {
+        unsigned char *raw =
+            reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
+        data = reinterpret_cast<uint32_t *>(raw);
+        win = reinterpret_cast<int *>(raw + Sh::kWinOffset);
+        full = reinterpret_cast<uint64_t *>(raw + Sh::kBarOffset);
+    }
+};
+
+// One output tile (TX x TY pixels x ZT slices) over all angles.  `g` counts
+// the angle blocks this CTA has already staged through the S-slot ring, so
+// one CTA can run many tiles back to back (slot = running block % S, barrier
+// parity = (running block / S) & 1).  Returns false if a bounded wait gave up.
 template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
-__global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUtensorMap map, const BPArgs args)
+__device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &args, int x0, int y0, int z0,
+                                        const BPSmem<BPShape<TX, TY, ZT, A, S>> &sm, uint32_t &g)
 {
     using Sh = BPShape<TX, TY, ZT, A, S>;
     constexpr int WIN = Sh::kWin;
@@ -238,28 +250,19 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
     constexpr int YSTEP = 256 / TX;
     constexpr bool PAIRS = KIND != SINO_F32;
     constexpr int ASTR = Sh::kAngleStride;
-    extern __shared__ __align__(128) unsigned char smem_dyn[];
-    unsigned char *smem_raw =
-        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~(uintptr_t)127);
-    uint32_t *data = reinterpret_cast<uint32_t *>(smem_raw);  // [S][A][ASTR], angle box = [ZT][WIN]
-    int *win = reinterpret_cast<int *>(smem_raw + Sh::kWinOffset);
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + Sh::kBarOffset);
+    uint32_t *data = sm.data;
+    int *win = sm.win;
+    uint64_t *full = sm.full;
 
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * ZT;
     const uint32_t P = args.P;
     const int nblk = (int)((P + A - 1) / A);
     const float axis = args.axis;
+    const uint32_t g0 = g;
 
-    if (tid == 0) {
-        for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-
-    // Producer: stage block `blk` into slot blk % S.
+    // Producer: stage block `blk` of this tile into slot (g0 + blk) % S.
     auto issue = [&](int blk) {
-        const int slot = blk % S;
+        const int slot = (int)((g0 + (uint32_t)blk) % S);
         const int p0 = blk * A;
         const int nval = min(A, (int)P - p0);
         mbar_arrive_expect_tx(&full[slot], (uint32_t)(nval * ZT * WIN * 4));
@@ -277,7 +280,7 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
             e = max(min(e, 1 << 24), -(1 << 24));
             const int xs = e & ~3;  // 16-byte aligned TMA x coordinate (floor for negatives)
             win[slot * A + a] = xs;
-            tma_load_3d(data + (size_t)(slot * A + a) * ASTR, &map, &full[slot], xs, p0 + a, z0);
+            tma_load_3d(data + (size_t)(slot * A + a) * ASTR, map, &full[slot], xs, p0 + a, z0);
         }
     };
 
@@ -303,8 +306,8 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
 
     for (int blk = 0; blk < nblk; blk++) {
         if (tid == 0 && blk + S - 1 < nblk) issue(blk + S - 1);
-        const int slot = blk % S;
-        const uint32_t parity = (uint32_t)((blk / S) & 1);
+        const int slot = (int)((g0 + (uint32_t)blk) % S);
+        const uint32_t parity = ((g0 + (uint32_t)blk) / S) & 1u;
         const bool ok = mbar_wait_bounded(&full[slot], parity, kWaitLimitNs);
         const int p0 = blk * A;
         const int nval = min(A, (int)P - p0);
@@ -391,8 +394,9 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
                 for (int k = 0; k < 2; k++) mbar_wait_bounded(&full[s], (uint32_t)k, kWaitLimitNs / 8);
             }
         }
-        return;
+        return false;
     }
+    g = g0 + (uint32_t)nblk;
 
     const float norm = args.norm;
 #pragma unroll
@@ -405,6 +409,58 @@ __global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUten
             if (z0 + z >= (int)args.nz) break;
             args.out[((size_t)(z0 + z) * args.roi_h + y) * args.roi_w + x] = acc[j][z] * norm;
         }
+    }
+    return true;
+}
+
+template <int S>
+__device__ __forceinline__ void init_ring(uint64_t *full)
+{
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) mbar_init(&full[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+}
+
+template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
+__global__ void __launch_bounds__(256) k_bp_linear(const __grid_constant__ CUtensorMap map, const BPArgs args)
+{
+    using Sh = BPShape<TX, TY, ZT, A, S>;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    const BPSmem<Sh> sm(smem_dyn);
+    init_ring<S>(sm.full);
+    uint32_t g = 0;
+    bp_tile<TX, TY, ZT, A, S, KIND, KAHAN>(&map, args, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * ZT, sm, g);
+}
+
+// ------------------------------------------------------------------ persistent batch kernel
+
+// Work item = (job, tile); items are ordered by decreasing cost (largest
+// angle count first) and taken dynamically from a device counter, so the
+// CTAs of one persistent launch balance jobs of very different sizes.
+template <int TX, int TY, int A, int S, int KIND, bool KAHAN>
+__global__ void __launch_bounds__(256) k_bp_batch(const BatchBP *__restrict__ jobs, const uint2 *__restrict__ items,
+                                                  uint32_t n_items, uint32_t *__restrict__ counter)
+{
+    using Sh = BPShape<TX, TY, 1, A, S>;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    const BPSmem<Sh> sm(smem_dyn);
+    __shared__ uint32_t s_item;
+    init_ring<S>(sm.full);
+    uint32_t g = 0;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        __syncthreads();
+        if (it >= n_items) break;
+        const uint2 w = items[it];  // (job, tile index)
+        const BatchBP *j = jobs + w.x;
+        const int tx = (int)(w.y % j->tiles_x), ty = (int)(w.y / j->tiles_x);
+        if (threadIdx.x == 0)
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&j->map) : "memory");
+        if (!bp_tile<TX, TY, 1, A, S, KIND, KAHAN>(&j->map, j->args, tx * TX, ty * TY, 0, sm, g)) break;
     }
 }
 
@@ -500,6 +556,73 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
     case 7: return launch_linear<32, 16, 4, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     default: return fail(UFOB_ERR_INVALID, "backproject: unknown tile id %d", tile);
     }
+}
+
+// ------------------------------------------------------------------ batch dispatch
+
+// Tile-shape variants of the persistent batch kernel (single slices, ZT = 1):
+// (tile height, angles per stage).  The autotuner picks one per batch.
+static const int kBatchVariants[][2] = {{16, 32}, {32, 16}, {8, 32}, {16, 16}};
+
+int bp_batch_variants() { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
+
+template <int TY, int A>
+static int batch_window()
+{
+    return BPShape<32, TY, 1, A, 3>::kWin;
+}
+
+void bp_batch_tile(int v, int *tx, int *ty, int *window)
+{
+    *tx = 32;
+    *ty = kBatchVariants[v][0];
+    switch (v) {
+    case 0: *window = batch_window<16, 32>(); break;
+    case 1: *window = batch_window<32, 16>(); break;
+    case 2: *window = batch_window<8, 32>(); break;
+    default: *window = batch_window<16, 16>(); break;
+    }
+}
+
+template <int TY, int A, int KIND, bool KAHAN>
+static ufob_status launch_batch_t(const BatchBP *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t *counter,
+                                  cudaStream_t s)
+{
+    using Sh = BPShape<32, TY, 1, A, 3>;
+    auto kern = k_bp_batch<32, TY, A, 3, KIND, KAHAN>;
+    UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
+    int per_sm = 0;
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, Sh::kSmem));
+    if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "backproject batch: kernel does not fit on an SM");
+    const uint32_t grid = std::min<uint32_t>((uint32_t)num_sms() * (uint32_t)per_sm, n_items);
+    if (!grid) return UFOB_OK;
+    kern<<<grid, 256, Sh::kSmem, s>>>(d_jobs, d_items, n_items, counter);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+template <int KIND, bool KAHAN>
+static ufob_status batch_variant(int v, const BatchBP *j, const uint2 *it, uint32_t n, uint32_t *c, cudaStream_t s)
+{
+    switch (v) {
+    case 0: return launch_batch_t<16, 32, KIND, KAHAN>(j, it, n, c, s);
+    case 1: return launch_batch_t<32, 16, KIND, KAHAN>(j, it, n, c, s);
+    case 2: return launch_batch_t<8, 32, KIND, KAHAN>(j, it, n, c, s);
+    case 3: return launch_batch_t<16, 16, KIND, KAHAN>(j, it, n, c, s);
+    default: return fail(UFOB_ERR_INVALID, "backproject batch: unknown variant %d", v);
+    }
+}
+
+ufob_status bp_batch_launch(const BatchBP *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t *d_counter,
+                            SinoKind kind, bool kahan, int variant, cudaStream_t s)
+{
+    if (kind == SINO_F32) return batch_variant<SINO_F32, false>(variant, d_jobs, d_items, n_items, d_counter, s);
+    if (kind == SINO_F16_PAIRS)
+        return kahan ? batch_variant<SINO_F16_PAIRS, true>(variant, d_jobs, d_items, n_items, d_counter, s)
+                     : batch_variant<SINO_F16_PAIRS, false>(variant, d_jobs, d_items, n_items, d_counter, s);
+    return kahan ? batch_variant<SINO_BF16_PAIRS, true>(variant, d_jobs, d_items, n_items, d_counter, s)
+                 : batch_variant<SINO_BF16_PAIRS, false>(variant, d_jobs, d_items, n_items, d_counter, s);
 }
 
 static int default_tile(const BPGeometry &g)

@@ -283,6 +283,58 @@ __device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
     }
 }
 
+// Filter rows 2*pair and 2*pair+1 (one complex FFT of a + i b) in shared memory.
+template <int OUT>
+__device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32_t width, uint32_t rows,
+                                            uint32_t in_pitch, uint32_t pair, float2 *bufA, float2 *bufB,
+                                            const float2 *tw, const float2 *gains, uint32_t N, int log2N,
+                                            void *__restrict__ out, uint32_t out_w, uint32_t out_pitch)
+{
+    const uint32_t ra = 2 * pair, rb = 2 * pair + 1;
+    const bool hasb = rb < rows;
+    const float *pa = in + (size_t)ra * in_pitch;
+    const float *pb = in + (size_t)rb * in_pitch;
+    __syncthreads();  // previous pair's output reads of bufA/bufB (and table loads) are done
+    for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
+        float a = 0.f, b = 0.f;
+        if (n < width) {
+            a = __ldg(pa + n);
+            if (hasb) b = __ldg(pb + n);
+        }
+        bufA[n] = make_float2(a, b);
+    }
+    __syncthreads();
+    float2 *Z = fft_smem<false>(bufA, bufB, tw, N, log2N);
+    // separate, filter, recombine (pairs (k, N-k) are disjoint across threads)
+    for (uint32_t k = threadIdx.x; k <= N / 2; k += blockDim.x) {
+        const uint32_t m = (N - k) & (N - 1);
+        float2 zk = Z[k], zm = Z[m], g = gains[k];
+        float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
+        float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
+        ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
+        Z[k] = make_float2(ax - by, ay + bx);
+        if (m != k) Z[m] = make_float2(ax + by, bx - ay);
+    }
+    __syncthreads();
+    float2 *other = (Z == bufA) ? bufB : bufA;
+    float2 *X = fft_smem<true>(Z, other, tw, N, log2N);
+    if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
+        uint32_t *o = reinterpret_cast<uint32_t *>(out);
+        for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
+            float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
+            float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
+            o[(size_t)ra * out_pitch + j] = pack_pair<OUT>(lo.x, hi.x);
+            if (hasb) o[(size_t)rb * out_pitch + j] = pack_pair<OUT>(lo.y, hi.y);
+        }
+    } else {
+        for (uint32_t n = threadIdx.x; n < out_w; n += blockDim.x) {
+            float2 v = X[n];
+            store_value<OUT>(out, (size_t)ra * out_pitch + n, v.x);
+            if (hasb) store_value<OUT>(out, (size_t)rb * out_pitch + n, v.y);
+        }
+    }
+}
+
 template <int OUT>
 __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__restrict__ in, uint32_t width,
                                                                 uint32_t rows, uint32_t in_pitch,
@@ -301,50 +353,40 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__r
     for (uint32_t i = threadIdx.x; i <= N / 2; i += blockDim.x) gains[i] = g_gains[i];
 
     const uint32_t npairs = (rows + 1) / 2;
-    for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
-        const uint32_t ra = 2 * pair, rb = 2 * pair + 1;
-        const bool hasb = rb < rows;
-        const float *pa = in + (size_t)ra * in_pitch;
-        const float *pb = in + (size_t)rb * in_pitch;
-        __syncthreads();  // previous pair's output reads of bufA/bufB are done
-        for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
-            float a = 0.f, b = 0.f;
-            if (n < width) {
-                a = __ldg(pa + n);
-                if (hasb) b = __ldg(pb + n);
-            }
-            bufA[n] = make_float2(a, b);
-        }
+    for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x)
+        filter_pair<OUT>(in, width, rows, in_pitch, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch);
+}
+
+// Persistent filter stage of an uneven batch: work items (job, row pair) are
+// grouped by FFT width and taken from a device counter; a CTA reloads its
+// shared twiddles/gains only when the width changes between its items.
+template <int OUT>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_batch(const BatchFilter *__restrict__ jobs,
+                                                                 const uint2 *__restrict__ items, uint32_t n_items,
+                                                                 uint32_t maxN, uint32_t *__restrict__ counter)
+{
+    extern __shared__ float4 smem_f4[];
+    float2 *bufA = reinterpret_cast<float2 *>(smem_f4);
+    float2 *bufB = bufA + maxN;
+    float2 *tw = bufB + maxN;
+    float2 *gains = tw + maxN;
+    __shared__ uint32_t s_item;
+    const float2 *loaded = nullptr;
+    while (true) {
         __syncthreads();
-        float2 *Z = fft_smem<false>(bufA, bufB, tw, N, log2N);
-        // separate, filter, recombine (pairs (k, N-k) are disjoint across threads)
-        for (uint32_t k = threadIdx.x; k <= N / 2; k += blockDim.x) {
-            const uint32_t m = (N - k) & (N - 1);
-            float2 zk = Z[k], zm = Z[m], g = gains[k];
-            float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
-            float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
-            ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
-            Z[k] = make_float2(ax - by, ay + bx);
-            if (m != k) Z[m] = make_float2(ax + by, bx - ay);
-        }
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1u);
         __syncthreads();
-        float2 *other = (Z == bufA) ? bufB : bufA;
-        float2 *X = fft_smem<true>(Z, other, tw, N, log2N);
-        if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
-            uint32_t *o = reinterpret_cast<uint32_t *>(out);
-            for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
-                float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
-                float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
-                o[(size_t)ra * out_pitch + j] = pack_pair<OUT>(lo.x, hi.x);
-                if (hasb) o[(size_t)rb * out_pitch + j] = pack_pair<OUT>(lo.y, hi.y);
-            }
-        } else {
-            for (uint32_t n = threadIdx.x; n < out_w; n += blockDim.x) {
-                float2 v = X[n];
-                store_value<OUT>(out, (size_t)ra * out_pitch + n, v.x);
-                if (hasb) store_value<OUT>(out, (size_t)rb * out_pitch + n, v.y);
-            }
+        const uint32_t it = s_item;
+        if (it >= n_items) break;
+        const uint2 w = items[it];  // (job, row pair)
+        const BatchFilter &j = jobs[w.x];
+        if (j.tw != loaded) {
+            for (uint32_t i = threadIdx.x; i < j.N; i += blockDim.x) tw[i] = j.tw[i];
+            for (uint32_t i = threadIdx.x; i <= j.N / 2; i += blockDim.x) gains[i] = j.gains[i];
+            loaded = j.tw;
         }
+        filter_pair<OUT>(j.in, j.width, j.rows, j.in_pitch, w.y, bufA, bufB, tw, gains, j.N, j.log2N, j.out, j.out_w,
+                         j.out_pitch);
     }
 }
 
@@ -420,6 +462,35 @@ ufob_status filter_spectrum_launch(const float *d_coeff, const float *d_in, floa
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
+}
+
+template <int OUT>
+static ufob_status launch_batch(const BatchFilter *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t maxN,
+                                uint32_t *d_counter, cudaStream_t s)
+{
+    const size_t smem = sizeof(float2) * (3 * (size_t)maxN + maxN / 2 + 1);
+    UFOB_CUDA_TRY(cudaFuncSetAttribute(k_filter_batch<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_batch<OUT>, kFilterThreads, smem));
+    if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", maxN);
+    uint32_t grid = std::min<uint32_t>((uint32_t)num_sms() * (uint32_t)per_sm, n_items);
+    if (!grid) return UFOB_OK;
+    k_filter_batch<OUT><<<grid, kFilterThreads, smem, s>>>(d_jobs, d_items, n_items, maxN, d_counter);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+ufob_status filter_batch_launch(const BatchFilter *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t maxN,
+                                uint32_t *d_counter, int out_kind, cudaStream_t s)
+{
+    if (maxN > kMaxFusedFFT) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u above %u", maxN, kMaxFusedFFT);
+    switch (out_kind) {
+    case OUT_F32: return launch_batch<OUT_F32>(d_jobs, d_items, n_items, maxN, d_counter, s);
+    case OUT_F16_PAIRS: return launch_batch<OUT_F16_PAIRS>(d_jobs, d_items, n_items, maxN, d_counter, s);
+    case OUT_BF16_PAIRS: return launch_batch<OUT_BF16_PAIRS>(d_jobs, d_items, n_items, maxN, d_counter, s);
+    default: return fail(UFOB_ERR_INVALID, "filter batch: unsupported output kind %d", out_kind);
+    }
 }
 
 }  // namespace ufob

@@ -82,9 +82,114 @@ __global__ void k_ellipsoid_stack(const double *__restrict__ ell, uint32_t n, ui
     }
 }
 
+// Ray-marching forward projector, src/kernels/forwardproject.cl:24-58: for
+// detector pixel idx and angle idy*step, walk unit steps along the ray through
+// the circle of radius min(axis, W - axis) and sum linear samples (texel
+// centres at +0.5, zero outside the image).  Exact FP32 weights; the angle's
+// sin/cos are taken in FP64.
+__global__ void k_forwardproject(const float *__restrict__ img, uint32_t W, uint32_t n_angles, float axis,
+                                 double step, float *__restrict__ sino)
+{
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x, idy = blockIdx.y;
+    if (idx >= W || idy >= n_angles) return;
+    double sd, cd;
+    sincos((double)idy * step, &sd, &cd);
+    const float r = fminf(axis, (float)W - axis);
+    const float d = (float)idx - axis + 0.5f;
+    const float l = sqrtf(4.0f * r * r - 4.0f * d * d);  // NaN outside the circle: no samples
+    float Dx = (float)cd, Dy = (float)sd;
+    const float nrm = rsqrtf(Dx * Dx + Dy * Dy);
+    Dx *= nrm;
+    Dy *= nrm;
+    const float Nx = Dy, Ny = -Dx;
+    float sx = d * Dx - l / 2.0f * Nx + axis, sy = d * Dy - l / 2.0f * Ny + axis;
+    float sum = 0.f;
+    for (int i = 0; (float)i < l; i++) {
+        const float u = sx - 0.5f, v = sy - 0.5f;
+        const float fu = floorf(u), fv = floorf(v);
+        const float a = u - fu, b = v - fv;
+        const int i0 = (int)fu, j0 = (int)fv;
+        float t00 = 0.f, t10 = 0.f, t01 = 0.f, t11 = 0.f;
+        if (j0 >= 0 && j0 < (int)W) {
+            if (i0 >= 0 && i0 < (int)W) t00 = __ldg(img + (size_t)j0 * W + i0);
+            if (i0 + 1 >= 0 && i0 + 1 < (int)W) t10 = __ldg(img + (size_t)j0 * W + i0 + 1);
+        }
+        if (j0 + 1 >= 0 && j0 + 1 < (int)W) {
+            if (i0 >= 0 && i0 < (int)W) t01 = __ldg(img + (size_t)(j0 + 1) * W + i0);
+            if (i0 + 1 >= 0 && i0 + 1 < (int)W) t11 = __ldg(img + (size_t)(j0 + 1) * W + i0 + 1);
+        }
+        sum += (1.f - a) * (1.f - b) * t00 + a * (1.f - b) * t10 + (1.f - a) * b * t01 + a * b * t11;
+        sx += Nx;
+        sy += Ny;
+    }
+    sino[(size_t)idy * W + idx] = sum;
+}
+
+// Rasterise ellipse phantoms (cx, cy, a, b, phi, rho) at pixel centres with
+// ss x ss supersampling into a stack [n_images][N][N]; ellipse list i is
+// ell[offsets[i] .. offsets[i+1]).
+__global__ void k_ellipse_images(const Ellipse *__restrict__ ell, const uint32_t *__restrict__ offsets, uint32_t N,
+                                 double axis, double scale, int ss, float *__restrict__ out)
+{
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, im = blockIdx.z;
+    if (x >= N) return;
+    const uint32_t e0 = offsets[im], e1 = offsets[im + 1];
+    double acc = 0.0;
+    for (int sy = 0; sy < ss; sy++)
+        for (int sx = 0; sx < ss; sx++) {
+            const double px = ((double)x + (sx + 0.5) / ss - axis) / scale;
+            const double py = ((double)y + (sy + 0.5) / ss - axis) / scale;
+            for (uint32_t e = e0; e < e1; e++) {
+                const Ellipse q = ell[e];
+                double sp, cp;
+                sincos(q.phi, &sp, &cp);
+                const double dx = px - q.cx, dy = py - q.cy;
+                const double u = dx * cp + dy * sp, v = -dx * sp + dy * cp;
+                if (u * u / (q.a * q.a) + v * v / (q.b * q.b) <= 1.0) acc += q.rho;
+            }
+        }
+    out[((size_t)im * N + y) * N + x] = (float)(acc / (ss * ss));
+}
+
 }  // namespace ufob
 
 using namespace ufob;
+
+extern "C" ufob_status ufob_forwardproject(const float *d_slice, uint32_t width, uint32_t n_angles, double axis_pos,
+                                           double angle_step, float *d_sino, void *stream)
+{
+    if (!d_slice || !d_sino) return fail(UFOB_ERR_INVALID, "forwardproject: NULL argument");
+    if (!width || !n_angles) return fail(UFOB_ERR_INVALID, "forwardproject: empty size");
+    UFOB_TRY(ensure_device());
+    dim3 blk(128), grd((width + 127) / 128, n_angles);
+    k_forwardproject<<<grd, blk, 0, (cudaStream_t)stream>>>(d_slice, width, n_angles, (float)axis_pos, angle_step,
+                                                            d_sino);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_phantom_images(const double *h_ellipses, const uint32_t *h_offsets, uint32_t n_images,
+                                           uint32_t N, double axis, double scale, int supersample, float *d_out,
+                                           void *stream)
+{
+    if (!h_ellipses || !h_offsets || !d_out) return fail(UFOB_ERR_INVALID, "phantom_images: NULL argument");
+    if (supersample < 1 || supersample > 8) return fail(UFOB_ERR_INVALID, "phantom_images: supersample in [1, 8]");
+    UFOB_TRY(ensure_device());
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t n_ell = h_offsets[n_images];
+    DevBuf de, doff;
+    UFOB_TRY(de.ensure(sizeof(Ellipse) * (n_ell ? n_ell : 1)));
+    UFOB_TRY(doff.ensure(sizeof(uint32_t) * (n_images + 1)));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(de.ptr, h_ellipses, sizeof(Ellipse) * n_ell, cudaMemcpyHostToDevice, s));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(doff.ptr, h_offsets, sizeof(uint32_t) * (n_images + 1), cudaMemcpyHostToDevice, s));
+    k_ellipse_images<<<dim3((N + 127) / 128, N, n_images), 128, 0, s>>>(de.as<Ellipse>(), doff.as<uint32_t>(), N, axis,
+                                                                        scale, supersample, d_out);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    UFOB_CUDA_TRY(cudaStreamSynchronize(s));  // the staging buffers are freed on return
+    return UFOB_OK;
+}
 
 extern "C" ufob_status ufob_phantom_stack(const double *h_ell, uint32_t n, uint32_t W, uint32_t P, uint32_t nz,
                                           double angle_step, double axis, double scale, float *d_sino, void *stream)

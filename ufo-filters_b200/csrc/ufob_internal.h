@@ -1,6 +1,7 @@
 // Internal declarations shared by the engine's translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -97,6 +98,43 @@ enum SinoKind { SINO_F32 = 0, SINO_F16_PAIRS = 1, SINO_BF16_PAIRS = 2 };
 
 ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
                              uint64_t slice_pitch, float *d_out, bool kahan, int tile, cudaStream_t stream);
+
+// Kernel arguments of one backprojection (one stack or one batch job).
+struct BPArgs {
+    uint32_t P, nz;
+    uint32_t roi_x, roi_y, roi_w, roi_h;
+    float axis, norm;
+    const float2 *sincos;
+    float *out;
+    int *err;
+};
+
+// ------------------------------------------------------- uneven batches (persistent kernels)
+// One job of the filter stage: its rows, FFT width and tables.
+struct BatchFilter {
+    const float *in;
+    void *out;
+    const float2 *tw, *gains;
+    uint32_t width, rows, in_pitch, out_w, out_pitch, N;
+    int log2N;
+};
+// One job of the backprojection stage: tensor map (64-byte aligned, in global
+// memory), arguments and tile grid.
+struct alignas(64) BatchBP {
+    CUtensorMap map;
+    BPArgs args;
+    uint32_t tiles_x, tiles_y;
+};
+// filter stage over (job, row pair) items; out_kind: 0 F32 rows, 3 F16 pairs, 4 BF16 pairs
+ufob_status filter_batch_launch(const BatchFilter *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t maxN,
+                                uint32_t *d_counter, int out_kind, cudaStream_t s);
+// backprojection stage over (job, tile) items with tile-shape variant `variant`
+int bp_batch_variants();
+void bp_batch_tile(int variant, int *tx, int *ty, int *window);
+ufob_status bp_batch_launch(const BatchBP *d_jobs, const uint2 *d_items, uint32_t n_items, uint32_t *d_counter,
+                            SinoKind kind, bool kahan, int variant, cudaStream_t s);
+ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, uint32_t P, uint32_t nz,
+                          uint32_t pitch, uint64_t slice_pitch, uint32_t box_x, uint32_t box_z);
 ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t pitch, uint64_t slice_pitch,
                               float *d_out, cudaStream_t stream);
 

@@ -106,9 +106,12 @@ def lib():
             "ufob_batch_create": ([ctypes.POINTER(FilterProps), i, ctypes.POINTER(vp)], i),
             "ufob_batch_run": ([vp, ctypes.POINTER(Job), u32, vp], i),
             "ufob_batch_destroy": ([vp], None),
+            "ufob_batch_variant": ([vp], i),
             "ufob_phantom_sinogram": ([vp, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_phantom_stack": ([vp, u32, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_launch_count": ([], ctypes.c_uint64),
+            "ufob_forwardproject": ([vp, u32, u32, d, d, vp, vp], i),
+            "ufob_phantom_images": ([vp, vp, u32, u32, d, d, i, vp, vp], i),
             "ufob_measure_peaks": ([ctypes.POINTER(d), ctypes.POINTER(d)], i),
         }
         for name, (args, res) in sig.items():
@@ -423,6 +426,9 @@ class Batch:
                          j.get("axis_pos", -1.0), j.get("angle_step", -1.0), j.get("angle_offset", 0.0))
         check(lib().ufob_batch_run(self._h, arr, len(jobs), _stream(stream)))
 
+    def variant(self):
+        return int(lib().ufob_batch_variant(self._h))
+
     def __del__(self):
         if getattr(self, "_h", None):
             lib().ufob_batch_destroy(self._h)
@@ -479,3 +485,32 @@ def measure_peaks():
     a, b = ctypes.c_double(), ctypes.c_double()
     check(lib().ufob_measure_peaks(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def forwardproject(slice_img, n_angles, axis_pos=None, angle_step=None, out=None, stream=None):
+    """Ray-marching forward projection of a [W, W] CUDA tensor into [n_angles, W]."""
+    import torch
+    W = slice_img.shape[-1]
+    axis_pos = W / 2.0 if axis_pos is None else axis_pos
+    angle_step = math.pi / n_angles if angle_step is None else angle_step
+    img = slice_img.contiguous()
+    out = torch.empty((n_angles, W), dtype=torch.float32, device=img.device) if out is None else out
+    check(lib().ufob_forwardproject(_ptr(img), W, n_angles, axis_pos, angle_step, _ptr(out), _stream(stream)))
+    return out
+
+
+def phantom_images(ellipse_lists, N, axis=None, scale=None, supersample=4, stream=None):
+    """Rasterise a list of ellipse arrays into a [len(lists), N, N] CUDA tensor."""
+    import numpy as np
+    import torch
+    offs = np.zeros(len(ellipse_lists) + 1, dtype=np.uint32)
+    for i, e in enumerate(ellipse_lists):
+        offs[i + 1] = offs[i] + len(e)
+    ell = np.ascontiguousarray(np.concatenate([np.asarray(e, dtype=np.float64).reshape(-1, 6)
+                                               for e in ellipse_lists]), dtype=np.float64)
+    axis = N / 2.0 if axis is None else axis
+    scale = N / 2.0 if scale is None else scale
+    out = torch.empty((len(ellipse_lists), N, N), dtype=torch.float32, device="cuda")
+    check(lib().ufob_phantom_images(ell.ctypes.data, offs.ctypes.data, len(ellipse_lists), N, axis, scale,
+                                    supersample, _ptr(out), _stream(stream)))
+    return out
