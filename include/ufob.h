@@ -161,6 +161,26 @@ ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_
                                  uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream);
 void ufob_backproject_destroy(ufob_backproject *bp);
 
+/* Allocation-free backprojection (engine addition; it has no counterpart in
+ * the reference).  For callers that cannot allocate device memory: hosts that
+ * manage every byte of device memory in their own pool, acquisition pipelines
+ * that must not risk the device-wide synchronisation an allocation can imply,
+ * and code running while a stream is captured.  Same result as
+ * ufob_backproject_run() with the same properties, but stateless and without
+ * any cudaMalloc/cudaFree: the only scratch, the per-angle sin/cos table,
+ * lives in a fixed device array of UFOB_STATIC_MAX_ANGLES entries (256 KiB,
+ * held by every GPU that loads the library until the process exits).
+ *  - height (sinogram rows) must not exceed UFOB_STATIC_MAX_ANGLES;
+ *  - sinogram rows must be 16-byte aligned (no restaging);
+ *  - the first call on a device looks up the table's device address (set-up):
+ *    make it before any stream capture;
+ *  - all calls share the table and each rewrites it, so calls whose work
+ *    overlaps on the GPU (unordered streams) race. */
+#define UFOB_STATIC_MAX_ANGLES 32768
+ufob_status ufob_backproject_run_static(const ufob_bp_props *props, const void *d_sino, ufob_dtype sino_dtype,
+                                        ufob_layout sino_layout, uint32_t width, uint32_t height, uint32_t nslices,
+                                        uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream);
+
 /* ------------------------------------------------------------------- fbp
  * Whole `fft ! filter ! ifft ! backproject` chain for a stack of sinograms
  * [nslices][height][width] float32 -> [nslices][roi_h][roi_w] float32.

@@ -86,6 +86,7 @@ def lib():
             "ufob_backproject_get_requisition": ([vp, u32, u32, pu32, pu32], i),
             "ufob_backproject_run": ([vp, vp, i, i, u32, u32, u32, u32, u64, vp, vp], i),
             "ufob_backproject_destroy": ([vp], None),
+            "ufob_backproject_run_static": ([ctypes.POINTER(BPProps), vp, i, i, u32, u32, u32, u32, u64, vp, vp], i),
             "ufob_fbp_create": ([ctypes.POINTER(FilterProps), ctypes.POINTER(BPProps), i, ctypes.POINTER(vp)], i),
             "ufob_fbp_run": ([vp, vp, u32, u32, u32, vp, vp], i),
             "ufob_fbp_run_host": ([vp, vp, u32, u32, u32, vp, u32], i),
