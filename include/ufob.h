@@ -82,8 +82,12 @@ typedef enum {
 /* Layout of filtered output rows (engine extension, not a reference property). */
 typedef enum {
     UFOB_LAYOUT_ROWS = 0,  /* [rows][crop_width] of the output dtype */
-    UFOB_LAYOUT_PAIRS = 1  /* [rows][pair_stride] 32-bit pairs (s[j-1], s[j]), F16/BF16 only;
+    UFOB_LAYOUT_PAIRS = 1, /* [rows][pair_stride] 32-bit pairs (s[j-1], s[j]), F16/BF16 only;
                               pair_stride = round_up(crop_width + 1, 4) */
+    UFOB_LAYOUT_QUADS = 2  /* F16 only, for a stack of sinograms: [ceil(nslices/4)][height][cells]
+                              16-byte cells, cell j of group g holding the taps s[j-1], s[j] of
+                              slices 4g..4g+3 as halves (s0[j-1], s1[j-1], s2[j-1], s3[j-1],
+                              s0[j], s1[j], s2[j], s3[j]); cells >= crop_width + 1 */
 } ufob_layout;
 
 typedef struct {
@@ -113,6 +117,12 @@ ufob_status ufob_filter_get_requisition(ufob_filter *f, uint32_t width, uint32_t
 ufob_status ufob_filter_run(ufob_filter *f, const float *d_in, uint32_t width, uint32_t rows,
                             uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
                             uint32_t out_pitch, void *stream);
+/* Filter a stack [nslices][height][in_pitch] into the F16 QUADS layout
+ * (cells per row out_pitch, 0 = crop_width + 1), the input of the fastest
+ * half-precision backprojection. */
+ufob_status ufob_filter_run_quads(ufob_filter *f, const float *d_in, uint32_t width, uint32_t height,
+                                  uint32_t nslices, uint32_t in_pitch, void *d_out, uint32_t out_pitch,
+                                  void *stream);
 /* Host copy of the 2*nfft interleaved coefficients for an input of `width`. */
 ufob_status ufob_filter_coefficients(ufob_filter *f, uint32_t width, float *host_out, uint32_t n);
 /* The reference `filter` task alone: multiply complex-interleaved rows
@@ -141,6 +151,9 @@ typedef struct {
     int compensated;          /* blocked Kahan over angle blocks: 0 off, 1 on, -1 auto (>=1500 angles
                                  when the sinogram is stored as F16/BF16) */
     int tile;                 /* kernel shape id from the autotuner, -1 = automatic */
+    int half_sums;            /* F16 QUADS sinograms only: 0 (default) every product accumulated in
+                                 FP32; 1 interpolation and sums over blocks of 8 angles in packed
+                                 FP16, block sums accumulated in FP32 (faster, larger error) */
 } ufob_bp_props;
 
 typedef struct ufob_backproject ufob_backproject;
@@ -153,7 +166,9 @@ ufob_status ufob_backproject_get_requisition(ufob_backproject *bp, uint32_t widt
                                              uint32_t *out_width, uint32_t *out_height);
 /* Backproject `nslices` sinograms of `height` rows x `width` bins.
  * sino_dtype F32 with sino_layout ROWS (row pitch in floats, 0 = width), or
- * F16/BF16 with layout PAIRS as written by ufob_filter_run (pitch in pairs).
+ * F16/BF16 with layout PAIRS as written by ufob_filter_run (pitch in pairs), or
+ * F16 with layout QUADS as written by ufob_filter_run_quads (pitch in cells,
+ * slice_pitch = cells per group of four slices).
  * Sinogram z starts at d_sino + z * slice_pitch elements (0 = height * pitch).
  * Output slice z is [roi_height][roi_width] floats at d_out + z * roi_w * roi_h. */
 ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_dtype sino_dtype,
@@ -291,6 +306,44 @@ ufob_status ufob_forwardproject(const float *d_slice, uint32_t width, uint32_t n
  * supersample^2 samples per pixel. */
 ufob_status ufob_phantom_images(const double *h_ellipses, const uint32_t *h_offsets, uint32_t n_images, uint32_t N,
                                 double axis, double scale, int supersample, float *d_out, void *stream);
+/* ------------------------------------------------------------------- sparse-view CNN
+ * Engine addition with no counterpart in the reference: a 4-level U-Net
+ * (32/64/128/256 channels, 3x3 convolutions, BF16 weights and activations,
+ * FP32 accumulation on tcgen05 tensor cores) that corrects a 90-angle FBP slice
+ * toward the dense (1800-angle) reconstruction.  Images are [B][H][W] FP32 on
+ * the device, H and W multiples of 32 (4x space-to-depth, then 3 poolings).  Parameters/gradients/Adam moments are
+ * exchanged as one FP32 vector: per layer (16->32, 32->64, 64->128, 128->256,
+ * 256->128, 128->64, 64->32, 32->16) weights [Cout][9][Cin] then bias [Cout]. */
+typedef struct ufob_cnn ufob_cnn;
+ufob_status ufob_cnn_create(uint64_t seed, float scale, ufob_cnn **out);
+void ufob_cnn_destroy(ufob_cnn *net);
+/* out = fbp + scale * net(fbp / scale) */
+ufob_status ufob_cnn_forward(ufob_cnn *net, const float *d_fbp, float *d_out, int batch, int height, int width,
+                             void *stream);
+/* The same network through the training kernels (NHWC activations); the
+ * inference path above must agree with it to BF16 rounding. */
+ufob_status ufob_cnn_forward_nhwc(ufob_cnn *net, const float *d_fbp, float *d_out, int batch, int height, int width,
+                                  void *stream);
+/* One Adam step (beta 0.9/0.999) on the mean squared error against d_target;
+ * *loss_out (host, may be NULL) receives the loss before the step. */
+ufob_status ufob_cnn_train_step(ufob_cnn *net, const float *d_fbp, const float *d_target, int batch, int height,
+                                int width, float lr, double *loss_out, void *stream);
+uint64_t ufob_cnn_num_params(void);
+/* which: 0 parameters, 1 gradients of the last step (get only), 2 Adam m, 3 Adam v */
+ufob_status ufob_cnn_get_state(ufob_cnn *net, int which, float *h_values, uint64_t n);
+ufob_status ufob_cnn_set_state(ufob_cnn *net, int which, const float *h_values, uint64_t n);
+int64_t ufob_cnn_get_step(const ufob_cnn *net);
+ufob_status ufob_cnn_set_step(ufob_cnn *net, int64_t step);
+/* The network's convolution primitives (NHWC BF16 activations, weights
+ * [Cout][9][Cin] BF16, zero padding, tap t = 3*(dy+1) + (dx+1)).
+ * forward: out = relu?(conv(in, w) + bias + residual), written as BF16 (d_out)
+ * and/or FP32 (d_out_f32); channels multiples of 16 in [16, 256], Cin > 64 a
+ * multiple of 64.  wgrad: d_dw[Cout][9][Cin] += sum over pixels of dz x in (FP32). */
+ufob_status ufob_conv3x3_forward(const void *d_in, const void *d_w, const float *d_bias, const void *d_residual,
+                                 void *d_out, float *d_out_f32, int nb, int h, int w, int cin, int cout, int relu,
+                                 void *stream);
+ufob_status ufob_conv3x3_wgrad(const void *d_in, const void *d_dz, float *d_dw, int nb, int h, int w, int cin,
+                               int cout, void *stream);
 /* Number of engine kernels launched by this process so far. */
 uint64_t ufob_launch_count(void);
 /* Sustained shared-memory load bandwidth (GB/s, 32-bit conflict-free loads)

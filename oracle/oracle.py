@@ -489,3 +489,156 @@ def conv3x3_dgrad_weights(w):
     """Weights of the data-gradient convolution: [Cin][9][Cout], taps flipped."""
     w = np.asarray(w)
     return np.ascontiguousarray(w[:, ::-1, :].transpose(2, 1, 0))
+
+
+def bf16_round(x):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    f = np.asarray(x, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+# Layer table of the sparse-view correction network: (Cin, Cout, relu) for
+# enc1..enc4, dec3, dec2, dec1, out.  Must match cnn_net.cu.
+CNN_LAYERS = [(16, 32, 1), (32, 64, 1), (64, 128, 1), (128, 256, 1),
+              (256, 128, 1), (128, 64, 1), (64, 32, 1), (32, 16, 0)]
+
+
+def cnn_num_params():
+    return sum(co * 9 * ci + co for ci, co, _ in CNN_LAYERS)
+
+
+def cnn_unpack(params):
+    """Flat FP32 parameter vector -> [(w [Cout,9,Cin], b [Cout])]."""
+    out, off = [], 0
+    for ci, co, _ in CNN_LAYERS:
+        n = co * 9 * ci
+        w = np.asarray(params[off:off + n], dtype=np.float64).reshape(co, 9, ci)
+        off += n
+        b = np.asarray(params[off:off + co], dtype=np.float64)
+        off += co
+        out.append((w, b))
+    return out
+
+
+def cnn_pack(layers):
+    return np.concatenate([np.concatenate([w.ravel(), b.ravel()]) for w, b in layers])
+
+
+CNN_S = 4  # space-to-depth factor of the network input/output
+
+
+def _unshuffle(img):
+    """[B, 4H, 4W] -> [B, H, W, 16], channel 4*dy + dx."""
+    B, H4, W4 = img.shape
+    x = np.zeros((B, H4 // CNN_S, W4 // CNN_S, CNN_S * CNN_S))
+    for dy in range(CNN_S):
+        for dx in range(CNN_S):
+            x[..., CNN_S * dy + dx] = img[:, dy::CNN_S, dx::CNN_S]
+    return x
+
+
+def _shuffle(o):
+    """[B, H, W, 16] -> [B, 4H, 4W]."""
+    B, H, W, _ = o.shape
+    img = np.zeros((B, CNN_S * H, CNN_S * W))
+    for dy in range(CNN_S):
+        for dx in range(CNN_S):
+            img[:, dy::CNN_S, dx::CNN_S] = o[..., CNN_S * dy + dx]
+    return img
+
+
+def _pool(x):
+    return 0.25 * (x[:, 0::2, 0::2] + x[:, 0::2, 1::2] + x[:, 1::2, 0::2] + x[:, 1::2, 1::2])
+
+
+def _pool_grad(d):
+    return 0.25 * np.repeat(np.repeat(d, 2, axis=1), 2, axis=2)
+
+
+def _up(x):
+    return np.repeat(np.repeat(x, 2, axis=1), 2, axis=2)
+
+
+def _up_grad(d):
+    return d[:, 0::2, 0::2] + d[:, 0::2, 1::2] + d[:, 1::2, 0::2] + d[:, 1::2, 1::2]
+
+
+def cnn_forward(params, fbp, scale=1.0, bf16=False, keep=False):
+    """Forward pass of the correction network (restated from cnn_net.cu's
+    layer list): returns fbp + scale * shuffle(o[..., :4]).  With ``bf16`` the
+    weights and every stored activation are rounded to BF16 where the CUDA
+    engine stores BF16 (accumulation stays exact)."""
+    r = bf16_round if bf16 else (lambda v: np.asarray(v, dtype=np.float64))
+    fbp = np.asarray(fbp, dtype=np.float64)
+    L = [(r(w), b) for w, b in cnn_unpack(params)]
+    a = {}
+    a["x0"] = r(_unshuffle(np.asarray(fbp, dtype=np.float32) * np.float32(1.0 / scale)))
+    a["e1"] = r(conv3x3_nhwc(a["x0"], *L[0], relu=True))
+    a["p1"] = r(_pool(a["e1"]))
+    a["e2"] = r(conv3x3_nhwc(a["p1"], *L[1], relu=True))
+    a["p2"] = r(_pool(a["e2"]))
+    a["e3"] = r(conv3x3_nhwc(a["p2"], *L[2], relu=True))
+    a["p3"] = r(_pool(a["e3"]))
+    a["e4"] = r(conv3x3_nhwc(a["p3"], *L[3], relu=True))
+    a["d3"] = r(conv3x3_nhwc(a["e4"], *L[4], relu=True))
+    a["u3"] = r(_up(a["d3"]) + a["e3"])
+    a["d2"] = r(conv3x3_nhwc(a["u3"], *L[5], relu=True))
+    a["u2"] = r(_up(a["d2"]) + a["e2"])
+    a["d1"] = r(conv3x3_nhwc(a["u2"], *L[6], relu=True))
+    a["u1"] = r(_up(a["d1"]) + a["e1"])
+    a["o"] = conv3x3_nhwc(a["u1"], *L[7])
+    pred = fbp + scale * _shuffle(a["o"])
+    return (pred, a, L) if keep else pred
+
+
+def cnn_loss_and_grads(params, fbp, target, scale=1.0, bf16=False):
+    """MSE loss and its gradient with respect to the flat parameter vector
+    (FP64 backward of ``cnn_forward``; with ``bf16`` the per-layer output
+    gradients are rounded to BF16 where the CUDA engine rounds them)."""
+    r = bf16_round if bf16 else (lambda v: np.asarray(v, dtype=np.float64))
+    pred, a, L = cnn_forward(params, fbp, scale, bf16, keep=True)
+    target = np.asarray(target, dtype=np.float64)
+    n = pred.size
+    diff = pred - target
+    loss = float(np.mean(diff * diff))
+    dpred = 2.0 * diff / n
+    grads = [None] * 8
+
+    def layer(i, x, y, dy, want_dx=True):
+        dz = r(dy * (y > 0)) if CNN_LAYERS[i][2] else r(dy)
+        grads[i] = (conv3x3_wgrad_nhwc(x, dz), dz.sum(axis=(0, 1, 2)))
+        if want_dx:
+            return conv3x3_nhwc(dz, conv3x3_dgrad_weights(L[i][0]))
+        return None
+
+    dzo = r(_unshuffle(scale * dpred))
+    grads[7] = (conv3x3_wgrad_nhwc(a["u1"], dzo), dzo.sum(axis=(0, 1, 2)))
+    du1 = conv3x3_nhwc(dzo, conv3x3_dgrad_weights(L[7][0]))
+    g_e1 = du1.copy()
+    du2 = layer(6, a["u2"], a["d1"], _up_grad(du1))
+    g_e2 = du2.copy()
+    du3 = layer(5, a["u3"], a["d2"], _up_grad(du2))
+    g_e3 = du3.copy()
+    de4 = layer(4, a["e4"], a["d3"], _up_grad(du3))
+    dp3 = layer(3, a["p3"], a["e4"], de4)
+    g_e3 = g_e3 + _pool_grad(dp3)
+    dp2 = layer(2, a["p2"], a["e3"], g_e3)
+    g_e2 = g_e2 + _pool_grad(dp2)
+    dp1 = layer(1, a["p1"], a["e2"], g_e2)
+    g_e1 = g_e1 + _pool_grad(dp1)
+    layer(0, a["x0"], a["e1"], g_e1, want_dx=False)
+    return loss, cnn_pack(grads)
+
+
+def cnn_init(seed):
+    """He-initialised parameters (the engine initialises its own; this is for
+    CPU-side checks)."""
+    rng = np.random.default_rng(seed)
+    layers = []
+    for i, (ci, co, _) in enumerate(CNN_LAYERS):
+        w = rng.normal(0.0, math.sqrt(2.0 / (9.0 * ci)), size=(co, 9, ci))
+        b = rng.normal(0.0, 0.05, size=co)
+        layers.append((w, b))
+    return cnn_pack(layers).astype(np.float32)

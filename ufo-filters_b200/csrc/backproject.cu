@@ -464,6 +464,305 @@ __global__ void __launch_bounds__(256) k_bp_batch(const BatchBP *__restrict__ jo
     }
 }
 
+// ------------------------------------------------------------------ slice-quad FP16 kernel
+//
+// Storage form SINO_F16_QUADS, written by the filter stage for a stack: cell
+// (g, p, j) of 16 bytes carries both interpolation taps of the four slices
+// 4g..4g+3 at angle p,
+//   word 0 = (s0[j-1], s1[j-1])   word 1 = (s2[j-1], s3[j-1])
+//   word 2 = (s0[j],   s1[j])     word 3 = (s2[j],   s3[j])
+// for j = 0..W (taps outside the row are 0).  One 128-bit shared load then
+// feeds four updates, so the per-update instruction count is dominated by the
+// FMAs themselves.  The TMA box is (4 words, window, 1 angle, ZT/4 groups);
+// the window coordinate is not the innermost one and needs no alignment.
+//
+// The interpolation weight comes from the coordinate's fixed-point bits
+// (coordinate + 1.5 * 2^13 leaves 10 fractional bits in the FP32 mantissa),
+// assembled into the FP16 pair (1 + f, 1 + f) by one integer multiply-add and
+// turned into (f, f) and (1 - f, 1 - f) exactly by two packed FP16 ops: no
+// float-to-half conversion per update.  ACC selects how products are summed:
+//   QACC_F32  FP32 accumulation of every product (mixed fma.rn.f32.f16);
+//   QACC_LERP the lerp in packed FP16 (one rounding of the interpolated
+//             value), FP32 accumulation via mixed-precision adds;
+//   QACC_H16  lerp and sum of 8 consecutive angles in packed FP16, block
+//             sums accumulated in FP32.
+enum { QACC_F32 = 0, QACC_LERP = 1, QACC_H16 = 2 };
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// 4-D map over [groups][P][cells][4] 32-bit words; box = (4, box_cells, 1, box_groups).
+ufob_status make_quad_map(CUtensorMap *map, const void *base, uint32_t cells, uint32_t P, uint32_t groups,
+                          uint32_t pitch, uint64_t group_pitch, uint32_t box_cells, uint32_t box_groups)
+{
+    auto fn = encode_fn();
+    if (!fn) return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[4] = {4, cells, P, groups};
+    cuuint64_t strides[3] = {16, (cuuint64_t)pitch * 16, (cuuint64_t)group_pitch * 16};
+    cuuint32_t box[4] = {4, box_cells, 1, box_groups};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): cells=%u P=%u groups=%u pitch=%u box=%u,%u",
+                    (int)r, cells, P, groups, pitch, box_cells, box_groups);
+    return UFOB_OK;
+}
+
+template <int TX, int TY, int ZT, int A, int S>
+struct BPQShape {
+    static constexpr int kThreads = 256;
+    static constexpr int kRY = TY / (kThreads / TX);
+    static_assert(TX == 32 && ZT % 4 == 0, "one warp spans the tile width; whole slice groups");
+    static_assert(kRY >= 1 && kRY * (kThreads / TX) == TY, "tile height");
+    static constexpr int kSpan = (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
+    static constexpr int kWin = (kSpan + 2 + 2 + 1) / 2 * 2;  // + tap + guard on each side
+    static constexpr int kGroups = ZT / 4;
+    static constexpr int kAngleStride = (kGroups * kWin * 4 + 31) / 32 * 32;  // words; 128-byte aligned boxes
+    static constexpr int kStageElems = A * kAngleStride;
+    static constexpr size_t kDataBytes = (size_t)S * kStageElems * 4;
+    static constexpr size_t kWinOffset = kDataBytes;
+    static constexpr size_t kBarOffset = (kWinOffset + (size_t)S * A * 4 + 7) / 8 * 8;
+    static constexpr size_t kSmem = kBarOffset + (size_t)S * 8 + 128;
+};
+
+__device__ __forceinline__ uint32_t h2_fma(uint32_t a, uint32_t b, uint32_t c)
+{
+    uint32_t d;
+    asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+__device__ __forceinline__ uint32_t h2_mul(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+__device__ __forceinline__ uint32_t h2_add(uint32_t a, uint32_t b)
+{
+    uint32_t d;
+    asm("add.rn.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// (c0, c1) += (lo(x) * lo(w), hi(x) * lo(w)) with FP32 accumulation
+__device__ __forceinline__ void mix_fma2(float &c0, float &c1, uint32_t x, uint32_t w)
+{
+    asm("{\n\t.reg .b16 xl, xh, wl, wh;\n\tmov.b32 {xl, xh}, %2;\n\tmov.b32 {wl, wh}, %3;\n\t"
+        "fma.rn.f32.f16 %0, xl, wl, %0;\n\tfma.rn.f32.f16 %1, xh, wl, %1;\n\t}"
+        : "+f"(c0), "+f"(c1)
+        : "r"(x), "r"(w));
+}
+
+// (c0, c1) += (lo(x), hi(x)) with FP32 accumulation
+__device__ __forceinline__ void mix_add2(float &c0, float &c1, uint32_t x)
+{
+    asm("{\n\t.reg .b16 xl, xh;\n\tmov.b32 {xl, xh}, %2;\n\t"
+        "add.rn.f32.f16 %0, xl, %0;\n\tadd.rn.f32.f16 %1, xh, %1;\n\t}"
+        : "+f"(c0), "+f"(c1)
+        : "r"(x));
+}
+
+__device__ __forceinline__ void h2_flush(float &c0, float &c1, uint32_t &h)
+{
+    mix_add2(c0, c1, h);
+    h = 0u;
+}
+
+template <int TX, int TY, int ZT, int A, int S, int ACC, bool KAHAN>
+__device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPArgs &args, int x0, int y0, int z0,
+                                              const BPSmem<BPQShape<TX, TY, ZT, A, S>> &sm, uint32_t &g)
+{
+    using Sh = BPQShape<TX, TY, ZT, A, S>;
+    constexpr int WIN = Sh::kWin;
+    constexpr int RY = Sh::kRY;
+    constexpr int NG = Sh::kGroups;
+    constexpr int YSTEP = 256 / TX;
+    constexpr int ASTR = Sh::kAngleStride;
+    constexpr int KB = ACC == QACC_H16 ? 8 : A;  // angles per FP16 block sum (QACC_H16)
+    uint32_t *data = sm.data;
+    int *win = sm.win;
+    uint64_t *full = sm.full;
+
+    const int tid = threadIdx.x;
+    const uint32_t P = args.P;
+    const int nblk = (int)((P + A - 1) / A);
+    const float axis = args.axis;
+    const uint32_t g0 = g;
+
+    auto issue = [&](int blk) {
+        const int slot = (int)((g0 + (uint32_t)blk) % S);
+        const int p0 = blk * A;
+        const int nval = min(A, (int)P - p0);
+        mbar_arrive_expect_tx(&full[slot], (uint32_t)(nval * NG * WIN * 16));
+        const float cx0 = (float)(args.roi_x + x0) - axis + 0.5f, cx1 = cx0 + (float)(TX - 1);
+        const float cy0 = (float)(args.roi_y + y0) - axis + 0.5f, cy1 = cy0 + (float)(TY - 1);
+        for (int a = 0; a < nval; a++) {
+            const float2 sc = args.sincos[p0 + a];
+            float h0 = fmaf(cy0, sc.x, fmaf(cx0, sc.y, axis));
+            float h1 = fmaf(cy0, sc.x, fmaf(cx1, sc.y, axis));
+            float h2 = fmaf(cy1, sc.x, fmaf(cx0, sc.y, axis));
+            float h3 = fmaf(cy1, sc.x, fmaf(cx1, sc.y, axis));
+            float hmin = fminf(fminf(h0, h1), fminf(h2, h3));
+            // first cell needed: floor(hmin - 0.5) + 1, minus one guard cell
+            int e = (int)floorf(hmin - 0.5f);
+            e = max(min(e, 1 << 24), -(1 << 24));
+            win[slot * A + a] = e;
+            tma_load_4d(data + (size_t)(slot * A + a) * ASTR, map, &full[slot], 0, e, p0 + a, z0 / 4);
+        }
+    };
+
+    if (tid == 0)
+        for (int b = 0; b < S - 1 && b < nblk; b++) issue(b);
+
+    const int lx = tid % TX, ly = tid / TX;
+    const float bx = (float)(args.roi_x + x0 + lx) - axis + 0.5f;
+    float by[RY];
+#pragma unroll
+    for (int j = 0; j < RY; j++) by[j] = (float)(args.roi_y + y0 + ly + j * YSTEP) - axis + 0.5f;
+
+    float acc[RY][ZT], comp[RY][ZT];
+#pragma unroll
+    for (int j = 0; j < RY; j++)
+#pragma unroll
+        for (int z = 0; z < ZT; z++) acc[j][z] = comp[j][z] = 0.f;
+
+    const float kFix = 12288.0f;  // 1.5 * 2^13: 10 fractional bits left in the mantissa
+    const uint32_t kFixBits = __float_as_uint(kFix);
+    const float toff = axis + 0.5f;  // cell coordinate = h - 0.5 + 1 - window origin
+    bool aborted = false;
+
+    for (int blk = 0; blk < nblk; blk++) {
+        if (tid == 0 && blk + S - 1 < nblk) issue(blk + S - 1);
+        const int slot = (int)((g0 + (uint32_t)blk) % S);
+        const uint32_t parity = ((g0 + (uint32_t)blk) / S) & 1u;
+        const bool ok = mbar_wait_bounded(&full[slot], parity, kWaitLimitNs);
+        const int p0 = blk * A;
+        const int nval = min(A, (int)P - p0);
+        const uint32_t *sdata = data + (size_t)slot * A * ASTR;
+
+        float part[RY][ZT];
+#pragma unroll
+        for (int j = 0; j < RY; j++)
+#pragma unroll
+            for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
+
+        if (ok) {
+            for (int a0 = 0; a0 < nval; a0 += KB) {
+                uint32_t hs[RY][ZT / 2];
+#pragma unroll
+                for (int j = 0; j < RY; j++)
+#pragma unroll
+                    for (int q = 0; q < ZT / 2; q++) hs[j][q] = 0u;
+                const int a1 = min(a0 + KB, nval);
+#pragma unroll 2
+                for (int a = a0; a < a1; a++) {
+                    const float2 sc = __ldg(&args.sincos[p0 + a]);
+                    const int xs = win[slot * A + a];
+                    const float t = fmaf(bx, sc.y, toff - (float)xs);
+                    const uint32_t *row = sdata + a * ASTR;
+#pragma unroll
+                    for (int j = 0; j < RY; j++) {
+                        const float u = fmaf(by[j], sc.x, t);
+                        const uint32_t bits = __float_as_uint(u + kFix);
+                        const uint32_t e = min((uint32_t)((int)(bits - kFixBits) >> 10), (uint32_t)(WIN - 1));
+                        const uint32_t pat = (bits & 1023u) * 0x00010001u + 0x3C003C00u;  // (1 + f, 1 + f)
+                        const uint32_t whi = h2_add(pat, 0xBC00BC00u);                    // (f, f)
+                        const uint32_t wlo = h2_fma(pat, 0xBC00BC00u, 0x40004000u);       // (1 - f, 1 - f)
+#pragma unroll
+                        for (int q = 0; q < NG; q++) {
+                            const uint4 v = *reinterpret_cast<const uint4 *>(row + (q * WIN + (int)e) * 4);
+                            float *pz = &part[j][4 * q];
+                            if (ACC == QACC_F32) {
+                                mix_fma2(pz[0], pz[1], v.x, wlo);
+                                mix_fma2(pz[0], pz[1], v.z, whi);
+                                mix_fma2(pz[2], pz[3], v.y, wlo);
+                                mix_fma2(pz[2], pz[3], v.w, whi);
+                            } else if (ACC == QACC_LERP) {
+                                mix_add2(pz[0], pz[1], h2_fma(v.z, whi, h2_mul(v.x, wlo)));
+                                mix_add2(pz[2], pz[3], h2_fma(v.w, whi, h2_mul(v.y, wlo)));
+                            } else {
+                                hs[j][2 * q] = h2_fma(v.z, whi, h2_fma(v.x, wlo, hs[j][2 * q]));
+                                hs[j][2 * q + 1] = h2_fma(v.w, whi, h2_fma(v.y, wlo, hs[j][2 * q + 1]));
+                            }
+                        }
+                    }
+                }
+                if (ACC == QACC_H16) {
+#pragma unroll
+                    for (int j = 0; j < RY; j++)
+#pragma unroll
+                        for (int q = 0; q < ZT / 2; q++) h2_flush(part[j][2 * q], part[j][2 * q + 1], hs[j][q]);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < RY; j++)
+#pragma unroll
+            for (int z = 0; z < ZT; z++) {
+                if (KAHAN) {
+                    const float yk = part[j][z] - comp[j][z];
+                    const float tk = acc[j][z] + yk;
+                    comp[j][z] = (tk - acc[j][z]) - yk;
+                    acc[j][z] = tk;
+                } else {
+                    acc[j][z] += part[j][z];
+                }
+            }
+        if (__syncthreads_or(!ok)) {
+            aborted = true;
+            break;
+        }
+    }
+
+    if (aborted) {
+        if (tid == 0) {
+            atomicExch(args.err, kErrTmaTimeout);
+            for (int s = 0; s < S; s++) {
+                for (int k = 0; k < 2; k++) mbar_wait_bounded(&full[s], (uint32_t)k, kWaitLimitNs / 8);
+            }
+        }
+        return false;
+    }
+    g = g0 + (uint32_t)nblk;
+
+    const float norm = args.norm;
+#pragma unroll
+    for (int j = 0; j < RY; j++) {
+        const int y = y0 + ly + j * YSTEP;
+        const int x = x0 + lx;
+        if (y >= (int)args.roi_h || x >= (int)args.roi_w) continue;
+#pragma unroll
+        for (int z = 0; z < ZT; z++) {
+            if (z0 + z >= (int)args.nz) break;
+            args.out[((size_t)(z0 + z) * args.roi_h + y) * args.roi_w + x] = acc[j][z] * norm;
+        }
+    }
+    return true;
+}
+
+template <int TX, int TY, int ZT, int A, int S, int ACC, bool KAHAN>
+__global__ void __launch_bounds__(256) k_bp_quads(const __grid_constant__ CUtensorMap map, const BPArgs args)
+{
+    using Sh = BPQShape<TX, TY, ZT, A, S>;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    const BPSmem<Sh> sm(smem_dyn);
+    init_ring<S>(sm.full);
+    uint32_t g = 0;
+    bp_tile_quads<TX, TY, ZT, A, S, ACC, KAHAN>(&map, args, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * ZT, sm,
+                                                 g);
+}
+
 // ------------------------------------------------------------------ nearest kernel
 
 // backproject.cl:24-48: index the flat sinogram with the OUTPUT width as row
@@ -623,6 +922,85 @@ ufob_status bp_batch_launch(const BatchBP *d_jobs, const uint2 *d_items, uint32_
                      : batch_variant<SINO_F16_PAIRS, false>(variant, d_jobs, d_items, n_items, d_counter, s);
     return kahan ? batch_variant<SINO_BF16_PAIRS, true>(variant, d_jobs, d_items, n_items, d_counter, s)
                  : batch_variant<SINO_BF16_PAIRS, false>(variant, d_jobs, d_items, n_items, d_counter, s);
+}
+
+template <int TX, int TY, int ZT, int A, int S, int ACC, bool KAHAN>
+static ufob_status launch_quads_t(const BPGeometry &g, const void *d_sino, uint32_t pitch, uint64_t group_pitch,
+                                  float *d_out, cudaStream_t stream)
+{
+    using Sh = BPQShape<TX, TY, ZT, A, S>;
+    auto kern = k_bp_quads<TX, TY, ZT, A, S, ACC, KAHAN>;
+    static bool attr = false;
+    if (!attr) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
+        attr = true;
+    }
+    CUtensorMap map;
+    UFOB_TRY(make_quad_map(&map, d_sino, g.W + 1, g.P, (g.nz + 3) / 4, pitch, group_pitch, Sh::kWin, Sh::kGroups));
+    BPArgs a;
+    a.P = g.P;
+    a.nz = g.nz;
+    a.roi_x = g.roi_x;
+    a.roi_y = g.roi_y;
+    a.roi_w = g.roi_w;
+    a.roi_h = g.roi_h;
+    a.axis = g.axis;
+    a.norm = g.norm;
+    a.sincos = g.d_sincos;
+    a.out = d_out;
+    a.err = device_error_word();
+    dim3 grid((g.roi_w + TX - 1) / TX, (g.roi_h + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
+    kern<<<grid, Sh::kThreads, Sh::kSmem, stream>>>(map, a);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+template <int ACC, bool KAHAN>
+static ufob_status quads_tile(int tile, const BPGeometry &g, const void *d, uint32_t pitch, uint64_t gp, float *o,
+                              cudaStream_t s)
+{
+    switch (tile) {
+    case 0: return launch_quads_t<32, 16, 4, 16, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 1: return launch_quads_t<32, 32, 4, 16, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 2: return launch_quads_t<32, 16, 8, 16, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 3: return launch_quads_t<32, 32, 8, 16, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 4: return launch_quads_t<32, 16, 8, 32, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 5: return launch_quads_t<32, 8, 8, 32, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 6: return launch_quads_t<32, 32, 8, 32, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 7: return launch_quads_t<32, 16, 8, 32, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 8: return launch_quads_t<32, 16, 16, 16, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 9: return launch_quads_t<32, 16, 16, 8, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 10: return launch_quads_t<32, 8, 16, 16, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    default: return fail(UFOB_ERR_INVALID, "backproject: unknown slice-quad tile id %d", tile);
+    }
+}
+
+int bp_quad_tiles() { return 11; }
+
+// Slice-quad FP16 backprojection.  pitch = cells per angle row (>= W + 1),
+// group_pitch = cells per group of four slices (>= P * pitch).  `tile` < 0
+// picks the default shape; `acc` is one of QACC_*.
+ufob_status bp_quads_launch(const BPGeometry &g, const void *d_sino, uint32_t pitch, uint64_t group_pitch,
+                            float *d_out, bool kahan, int acc, int tile, cudaStream_t stream)
+{
+    if (!g.roi_w || !g.roi_h || !g.nz || !g.P) return UFOB_OK;
+    if ((uintptr_t)d_sino & 15) return fail(UFOB_ERR_INVALID, "backproject: slice-quad base must be 16-byte aligned");
+    if (pitch < g.W + 1 || group_pitch < (uint64_t)pitch * g.P)
+        return fail(UFOB_ERR_INVALID, "backproject: slice-quad pitches too small");
+    if (tile < 0) tile = g.nz <= 4 ? 0 : 2;
+    switch (acc) {
+    case QACC_F32:
+        return kahan ? quads_tile<QACC_F32, true>(tile, g, d_sino, pitch, group_pitch, d_out, stream)
+                     : quads_tile<QACC_F32, false>(tile, g, d_sino, pitch, group_pitch, d_out, stream);
+    case QACC_LERP:
+        return kahan ? quads_tile<QACC_LERP, true>(tile, g, d_sino, pitch, group_pitch, d_out, stream)
+                     : quads_tile<QACC_LERP, false>(tile, g, d_sino, pitch, group_pitch, d_out, stream);
+    case QACC_H16:
+        return kahan ? quads_tile<QACC_H16, true>(tile, g, d_sino, pitch, group_pitch, d_out, stream)
+                     : quads_tile<QACC_H16, false>(tile, g, d_sino, pitch, group_pitch, d_out, stream);
+    default: return fail(UFOB_ERR_INVALID, "backproject: unknown accumulation mode %d", acc);
+    }
 }
 
 static int default_tile(const BPGeometry &g)

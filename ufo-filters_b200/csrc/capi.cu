@@ -64,18 +64,25 @@ static std::atomic<uint64_t> g_launches{0};
 
 void note_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Checked once per device ordinal (cheap attribute queries; cudaGetDeviceProperties
+// costs milliseconds and must stay off the per-call path).
+static std::atomic<int> g_device_ok[64];
+
 ufob_status ensure_device()
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice (no usable CUDA device)");
-    cudaDeviceProp prop;
-    e = cudaGetDeviceProperties(&prop, dev);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
-    if (prop.major != 10)
-        return fail(UFOB_ERR_CUDA, "device %d (%s) is sm_%d%d; this engine is built for sm_100a only", dev, prop.name,
-                    prop.major, prop.minor);
-    g_num_sms = prop.multiProcessorCount;
+    if (dev >= 0 && dev < 64 && g_device_ok[dev].load(std::memory_order_acquire)) return UFOB_OK;
+    int major = 0, minor = 0, sms = 0;
+    e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
+    if (major != 10)
+        return fail(UFOB_ERR_CUDA, "device %d is sm_%d%d; this engine is built for sm_100a only", dev, major, minor);
+    g_num_sms = sms;
+    if (dev >= 0 && dev < 64) g_device_ok[dev].store(1, std::memory_order_release);
     return UFOB_OK;
 }
 
@@ -89,8 +96,16 @@ __device__ int g_device_error = 0;
 
 int *device_error_word()
 {
+    static std::atomic<int *> cached[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64) {
+        int *c = cached[dev].load(std::memory_order_acquire);
+        if (c) return c;
+    }
     void *p = nullptr;
     cudaGetSymbolAddress(&p, g_device_error);
+    if (dev >= 0 && dev < 64 && p) cached[dev].store(reinterpret_cast<int *>(p), std::memory_order_release);
     return reinterpret_cast<int *>(p);
 }
 
@@ -271,7 +286,24 @@ ufob_status ufob_filter_run(ufob_filter *f, const float *d_in, uint32_t width, u
     UFOB_TRY(filter_plan_build(f->props, n, f->plan, s));
     if (!in_pitch) in_pitch = width;
     if (!out_pitch) out_pitch = out_layout == UFOB_LAYOUT_PAIRS ? round_up(w + 1, 4) : w;
+    if (out_layout == UFOB_LAYOUT_QUADS)
+        return fail(UFOB_ERR_INVALID, "filter: the QUADS layout needs the stack shape: use ufob_filter_run_quads");
     return filter_rows_launch(f->plan, d_in, width, rows, in_pitch, d_out, out_dtype, out_layout, w, out_pitch, s);
+}
+
+ufob_status ufob_filter_run_quads(ufob_filter *f, const float *d_in, uint32_t width, uint32_t height,
+                                  uint32_t nslices, uint32_t in_pitch, void *d_out, uint32_t out_pitch, void *stream)
+{
+    if (!f || !d_in || !d_out) return fail(UFOB_ERR_INVALID, "filter_run_quads: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t n, w;
+    UFOB_TRY(filter_sizes(f->props, width, &n, &w));
+    cudaStream_t s = (cudaStream_t)stream;
+    UFOB_TRY(filter_plan_build(f->props, n, f->plan, s));
+    if (!in_pitch) in_pitch = width;
+    if (!out_pitch) out_pitch = w + 1;
+    if (!height || !nslices) return UFOB_OK;
+    return filter_quads_launch(f->plan, d_in, width, height, nslices, in_pitch, d_out, w, out_pitch, s);
 }
 
 ufob_status ufob_filter_coefficients(ufob_filter *f, uint32_t width, float *host_out, uint32_t count)
@@ -327,6 +359,7 @@ void ufob_bp_props_init(ufob_bp_props *p)
     p->roi_width = p->roi_height = 0;
     p->compensated = -1;
     p->tile = -1;
+    p->half_sums = 0;
 }
 
 static ufob_status validate_bp_props(const ufob_bp_props *p)
@@ -368,6 +401,7 @@ ufob_status ufob_backproject_set_property(ufob_backproject *bp, const char *name
     else if (prop_is(name, "roi-height")) p.roi_height = (uint32_t)std::max(0.0, v);
     else if (prop_is(name, "compensated")) p.compensated = (int)v;
     else if (prop_is(name, "tile")) p.tile = (int)v;
+    else if (prop_is(name, "half-sums")) p.half_sums = (int)v;
     else return fail(UFOB_ERR_INVALID, "backproject: no property named '%s'", name ? name : "(null)");
     if ((prop_is(name, "num-projections") || prop_is(name, "offset") || prop_is(name, "roi-x") ||
          prop_is(name, "roi-y") || prop_is(name, "roi-width") || prop_is(name, "roi-height")) && v < 0)
@@ -468,6 +502,21 @@ extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_
     cudaStream_t s = (cudaStream_t)stream;
     BPGeometry g;
     UFOB_TRY(bp_prepare(bp, width, height, nslices, g, s));
+    if (layout == UFOB_LAYOUT_QUADS) {
+        if (dtype != UFOB_F16) return fail(UFOB_ERR_INVALID, "backproject: the QUADS layout is F16 only");
+        if (bp->props.mode == UFOB_BP_NEAREST)
+            return fail(UFOB_ERR_INVALID, "backproject: mode=nearest needs an F32 sinogram");
+        if (!pitch) pitch = width + 1;
+        if (!slice_pitch) slice_pitch = (uint64_t)pitch * height;
+        // tile ids 16..23: the same shapes with the FP16-lerp accumulation (measurement aid)
+        int tile = bp->props.tile, acc = bp->props.half_sums ? 2 : 0;
+        if (tile >= 16) {
+            acc = 1;
+            tile -= 16;
+        }
+        return bp_quads_launch(g, d_sino, pitch, slice_pitch, d_out, want_kahan(bp->props, SINO_F16_PAIRS, height),
+                               acc, tile, s);
+    }
     SinoKind kind;
     if (dtype == UFOB_F32 && layout == UFOB_LAYOUT_ROWS) kind = SINO_F32;
     else if (dtype == UFOB_F16 && layout == UFOB_LAYOUT_PAIRS) kind = SINO_F16_PAIRS;
@@ -575,9 +624,12 @@ static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, u
     uint32_t nfft, fw;
     UFOB_TRY(filter_sizes(x->f->props, width, &nfft, &fw));
     UFOB_TRY(filter_plan_build(x->f->props, nfft, x->f->plan, s));
-    const bool pairs = x->storage != UFOB_F32;
-    const uint32_t pitch = pairs ? round_up(fw + 1, 4) : round_up(fw, 4);
-    UFOB_TRY(x->work.ensure((size_t)pitch * 4 * height * nz));
+    // F16: slice-quad cells (16 B per detector position and four slices); BF16: pairs; F32: rows
+    const bool quads = x->storage == UFOB_F16;
+    const bool pairs = x->storage == UFOB_BF16;
+    const uint32_t pitch = quads ? fw + 1 : pairs ? round_up(fw + 1, 4) : round_up(fw, 4);
+    const size_t work_bytes = quads ? (size_t)pitch * 16 * height * ((nz + 3) / 4) : (size_t)pitch * 4 * height * nz;
+    UFOB_TRY(x->work.ensure(work_bytes));
     cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
     if (x->timing) {
         e0 = x->next_event();
@@ -586,11 +638,15 @@ static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, u
         if (!e0 || !e1 || !e2) return fail(UFOB_ERR_CUDA, "fbp: cannot create timing events");
         UFOB_CUDA_TRY(cudaEventRecord(e0, s));
     }
-    UFOB_TRY(filter_rows_launch(x->f->plan, d_sino, width, height * nz, width, x->work.ptr, x->storage,
-                                pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw, pitch, s));
+    const ufob_layout layout = quads ? UFOB_LAYOUT_QUADS : pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS;
+    if (quads)
+        UFOB_TRY(filter_quads_launch(x->f->plan, d_sino, width, height, nz, width, x->work.ptr, fw, pitch, s));
+    else
+        UFOB_TRY(filter_rows_launch(x->f->plan, d_sino, width, height * nz, width, x->work.ptr, x->storage, layout, fw,
+                                    pitch, s));
     if (x->timing) UFOB_CUDA_TRY(cudaEventRecord(e1, s));
-    UFOB_TRY(ufob_backproject_run(x->bp, x->work.ptr, x->storage, pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS, fw,
-                                  height, nz, pitch, (uint64_t)pitch * height, d_out, s));
+    UFOB_TRY(ufob_backproject_run(x->bp, x->work.ptr, x->storage, layout, fw, height, nz, pitch,
+                                  (uint64_t)pitch * height, d_out, s));
     if (x->timing) {
         UFOB_CUDA_TRY(cudaEventRecord(e2, s));
         x->t_filter.emplace_back(e0, e1);

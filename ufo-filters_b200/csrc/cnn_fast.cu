@@ -1,0 +1,659 @@
+// Inference path of the sparse-view correction network: persistent,
+// warp-specialised tcgen05 convolutions over a padded channel-group layout.
+//
+// Activation layout "CG": a tensor of B images, H x W pixels, C channels is
+// stored as C/8 planes; plane g holds channels 8g..8g+7 of every pixel as one
+// 16-byte row, rows ordered by the flattened PADDED image index
+//   q = (b * (H + 2) + y + 1) * (W + 2) + x + 1,
+// preceded by guard rows and followed by a tail, all zero.  The
+// one-pixel zero border makes a 3x3 convolution a 1-D convolution over q with
+// the nine row offsets (dy * (W + 2) + dx), so for a tile of consecutive rows
+// the operand of every tap is the same staged halo block read at a different
+// start row: a K-major UMMA operand whose 8-row core matrices are 128
+// contiguous bytes.  Every load is therefore a plain 1-D bulk copy
+// (cp.async.bulk) of one plane's row range, and the weights, pre-arranged as
+// [tap][channel group][Cout][8], are one contiguous bulk copy per tap.
+//
+// CTA roles (192 threads): warp 0 lane 0 issues the bulk copies into an
+// A ring (halo blocks, 2 stages) and a B ring (per-tap weights, 4 stages);
+// warp 1 allocates tensor memory and lane 0 issues tcgen05.mma (M = 128 rows
+// per MMA, MT row blocks per tile, N = Cout, K = 16) and tcgen05.commit;
+// warps 2-5 drain the double-buffered accumulators (tcgen05.ld) and run the
+// fused epilogue: bias + ReLU + BF16 store, or the decoder's nearest 2x
+// up-sampling plus skip connection, or the output depth-to-space plus the
+// residual FBP image.  Border rows of the padded grid are never written, so
+// they stay zero.  Every mbarrier wait is bounded; on expiry the CTA raises a
+// shared abort flag, records an error code and winds down.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "ufob_internal.h"
+
+namespace ufob {
+
+typedef __nv_bfloat16 bf16;
+
+namespace {
+
+constexpr int kThreads = 192;
+constexpr int kAStages = 2;
+constexpr int kBStages = 4;
+constexpr int kErrFastTimeout = 0x2101;
+constexpr size_t kMaxSmem = 200 * 1024;
+constexpr uint64_t kLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t sa(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t *b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sa(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool bar_try(uint64_t *b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(sa(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t now_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait that also gives up as soon as another role raised the abort flag.
+__device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag)
+{
+    if (bar_try(b, parity)) return true;
+    const uint64_t t0 = now_ns();
+    while (!bar_try(b, parity)) {
+        if (*abort_flag) return false;
+        if (now_ns() - t0 > kLimitNs) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void bar_arrive(uint64_t *b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
+}
+
+__device__ __forceinline__ void bar_expect(uint64_t *b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sa(b)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *b)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sa(dst)),
+                 "l"(src), "r"(bytes), "r"(sa(b))
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t desc_kmajor(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+
+__host__ __device__ constexpr uint32_t idesc_f16_bf16(uint32_t M, uint32_t N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void commit(uint64_t *b)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(sa(b))
+                 : "memory");
+}
+
+__device__ __forceinline__ void ld8(uint32_t taddr, float (&v)[8])
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ uint4 pack8(const float (&v)[8])
+{
+    uint4 o;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+    for (int j = 0; j < 4; j++) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+    return o;
+}
+
+__device__ __forceinline__ void unpack8_add(const uint4 &u, float (&v)[8])
+{
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&u);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float2 f = __bfloat1622float2(h[j]);
+        v[2 * j] += f.x;
+        v[2 * j + 1] += f.y;
+    }
+}
+
+}  // namespace
+
+enum { EPI_STORE = 0, EPI_UPADD = 1, EPI_FINAL = 2 };
+
+// One padded-grid geometry (B images of H x W interior pixels).
+struct CGGeom {
+    int B, H, W;
+    long long rows;   // B * (H + 2) * (W + 2)
+    long long alloc;  // rows per plane including guard and tail
+    int guard;        // zero rows before q = 0
+};
+
+struct FastConvArgs {
+    const bf16 *in;   // CG, Cin channels, geometry gi
+    const bf16 *wt;   // [9][Cin/8][Cout][8]
+    const float *bias;
+    bf16 *out;        // EPI_STORE: CG at gi; EPI_UPADD: CG at 2x (go)
+    const bf16 *skip; // EPI_UPADD: CG at 2x (go)
+    const float *fbp; // EPI_FINAL: [B][4H][4W]
+    float *img;       // EPI_FINAL output
+    float scale;
+    CGGeom gi, go;
+    int Cin, Cout, MT, relu, mode;
+    long long ntiles;
+    int *err;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ uint64_t a_full[kAStages], a_empty[kAStages], b_full[kBStages], b_empty[kBStages];
+    __shared__ uint64_t t_full[2], t_empty[2];
+    __shared__ uint32_t tslot;
+    __shared__ int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int Cin = a.Cin, Cout = a.Cout, MT = a.MT;
+    const int cgc = Cin < 64 ? Cin / 8 : 8;  // channel groups per K chunk
+    const int nchunks = Cin / (cgc * 8);
+    const int Wp = a.gi.W + 2;
+    const int halo = Wp + 1;
+    const int arows = MT * 128 + 2 * halo;  // rows of one staged plane
+    const uint32_t a_plane = (uint32_t)arows * 16;
+    const uint32_t a_stage = a_plane * (uint32_t)cgc;
+    const uint32_t b_stage = (uint32_t)cgc * (uint32_t)Cout * 16;
+    unsigned char *sA = smem;
+    unsigned char *sB = smem + (size_t)kAStages * a_stage;
+    const uint32_t acc_cols = (uint32_t)(MT * Cout);
+    uint32_t ncols = 32;
+    while (ncols < 2 * acc_cols) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kAStages; i++) {
+            bar_init(&a_full[i], 1);
+            bar_init(&a_empty[i], 1);
+        }
+        for (int i = 0; i < kBStages; i++) {
+            bar_init(&b_full[i], 1);
+            bar_init(&b_empty[i], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            bar_init(&t_full[i], 1);
+            bar_init(&t_empty[i], 4);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(&tslot)), "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tslot;
+    volatile int *abort_p = &abort_flag;
+
+    // offsets of the nine taps in padded rows
+    const long long plane_elems = a.gi.alloc * 8;  // bf16 per input plane
+
+    if (warp == 0) {
+        if (lane == 0) {
+            uint32_t ka = 0, kb = 0;
+            int last_a[kAStages], last_b[kBStages];  // running index of each stage's last copy
+            for (int i = 0; i < kAStages; i++) last_a[i] = -1;
+            for (int i = 0; i < kBStages; i++) last_b[i] = -1;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
+                const long long q0 = tile * (long long)(MT * 128);
+                for (int kc = 0; kc < nchunks && ok; kc++) {
+                    const int s = (int)(ka % kAStages);
+                    ok = bar_wait(&a_empty[s], ((ka / kAStages) & 1u) ^ 1u, abort_p);
+                    if (!ok) break;
+                    bar_expect(&a_full[s], a_stage);
+                    for (int g = 0; g < cgc; g++) {
+                        const bf16 *src = a.in + (size_t)(kc * cgc + g) * plane_elems +
+                                          (size_t)(a.gi.guard + q0 - halo) * 8;
+                        bulk_g2s(sA + (size_t)s * a_stage + (size_t)g * a_plane, src, a_plane, &a_full[s]);
+                    }
+                    last_a[s] = (int)ka;
+                    ka++;
+                    for (int t = 0; t < 9 && ok; t++) {
+                        const int sb = (int)(kb % kBStages);
+                        ok = bar_wait(&b_empty[sb], ((kb / kBStages) & 1u) ^ 1u, abort_p);
+                        if (!ok) break;
+                        bar_expect(&b_full[sb], b_stage);
+                        const bf16 *src = a.wt + ((size_t)t * (Cin / 8) + (size_t)kc * cgc) * Cout * 8;
+                        bulk_g2s(sB + (size_t)sb * b_stage, src, b_stage, &b_full[sb]);
+                        last_b[sb] = (int)kb;
+                        kb++;
+                    }
+                }
+            }
+            if (!ok) {
+                atomicExch(a.err, kErrFastTimeout);
+                // let copies already in flight land before the CTA can exit (bounded)
+                for (int s = 0; s < kAStages; s++) {
+                    const uint64_t t0 = now_ns();
+                    if (last_a[s] >= 0)
+                        while (!bar_try(&a_full[s], ((uint32_t)last_a[s] / kAStages) & 1u) &&
+                               now_ns() - t0 < kLimitNs / 8) {
+                        }
+                }
+                for (int s = 0; s < kBStages; s++) {
+                    const uint64_t t0 = now_ns();
+                    if (last_b[s] >= 0)
+                        while (!bar_try(&b_full[s], ((uint32_t)last_b[s] / kBStages) & 1u) &&
+                               now_ns() - t0 < kLimitNs / 8) {
+                        }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_f16_bf16(128, (uint32_t)Cout);
+            uint32_t ka = 0, kb = 0, it = 0;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, it++) {
+                const uint32_t ab = it & 1u;
+                ok = bar_wait(&t_empty[ab], ((it >> 1) & 1u) ^ 1u, abort_p);
+                if (!ok) break;
+                fence_after();
+                const uint32_t dcol = tmem + ab * acc_cols;
+                for (int kc = 0; kc < nchunks && ok; kc++) {
+                    const int s = (int)(ka % kAStages);
+                    ok = bar_wait(&a_full[s], (ka / kAStages) & 1u, abort_p);
+                    if (!ok) break;
+                    fence_after();
+                    const uint32_t abase = sa(sA + (size_t)s * a_stage);
+                    for (int t = 0; t < 9 && ok; t++) {
+                        const int sb = (int)(kb % kBStages);
+                        ok = bar_wait(&b_full[sb], (kb / kBStages) & 1u, abort_p);
+                        if (!ok) break;
+                        fence_after();
+                        const uint32_t bbase = sa(sB + (size_t)sb * b_stage);
+                        const int off = halo + (t / 3 - 1) * Wp + (t % 3 - 1);
+                        for (int m = 0; m < MT; m++) {
+                            for (int k = 0; k < cgc / 2; k++) {
+                                const uint64_t da =
+                                    desc_kmajor(abase + (uint32_t)(off + m * 128) * 16 + (uint32_t)k * 2 * a_plane,
+                                                a_plane, 128);
+                                const uint64_t db =
+                                    desc_kmajor(bbase + (uint32_t)k * 2 * (uint32_t)Cout * 16, (uint32_t)Cout * 16, 128);
+                                mma(dcol + (uint32_t)(m * Cout), da, db, idesc, (kc | t | k) ? 1u : 0u);
+                            }
+                        }
+                        commit(&b_empty[sb]);  // frees the weight stage once these MMAs finish
+                        kb++;
+                    }
+                    commit(&a_empty[s]);
+                    ka++;
+                }
+                commit(&t_full[ab]);
+            }
+            if (!ok) atomicExch(a.err, kErrFastTimeout);
+        }
+    } else {
+        // epilogue warps 2..5: TMEM lane quarter = warp % 4
+        const int quarter = warp & 3;
+        uint32_t it = 0;
+        const int Hp = a.gi.H + 2;
+        const long long img_rows = (long long)Hp * Wp;
+        for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
+            const uint32_t ab = it & 1u;
+            if (!bar_wait(&t_full[ab], (it >> 1) & 1u, abort_p)) {
+                if (lane == 0) atomicExch(a.err, kErrFastTimeout);
+                break;
+            }
+            fence_after();
+            const long long q0 = tile * (long long)(MT * 128);
+            for (int m = 0; m < MT; m++) {
+                const long long q = q0 + m * 128 + quarter * 32 + lane;
+                const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + ab * acc_cols + (uint32_t)(m * Cout);
+                // interior test of this padded row
+                bool inside = q < a.gi.rows;
+                int b = 0, y = 0, x = 0;
+                if (inside) {
+                    b = (int)(q / img_rows);
+                    const int r = (int)(q - (long long)b * img_rows);
+                    y = r / Wp - 1;
+                    x = r - (y + 1) * Wp - 1;
+                    inside = y >= 0 && y < a.gi.H && x >= 0 && x < a.gi.W;
+                }
+                if (a.mode == EPI_FINAL) {
+                    // Cout = 16 = 4 x 4 sub-pixels: out = fbp + s * (acc + bias)
+                    float v[16];
+                    float t8[8];
+                    ld8(tbase, t8);
+#pragma unroll
+                    for (int j = 0; j < 8; j++) v[j] = t8[j];
+                    ld8(tbase + 8, t8);
+#pragma unroll
+                    for (int j = 0; j < 8; j++) v[8 + j] = t8[j];
+                    if (inside) {
+                        const int W4 = 4 * a.gi.W;
+                        const size_t base = ((size_t)b * 4 * a.gi.H + 4 * y) * W4 + 4 * x;
+#pragma unroll
+                        for (int dy = 0; dy < 4; dy++) {
+                            const float4 f = *reinterpret_cast<const float4 *>(a.fbp + base + (size_t)dy * W4);
+                            float4 o;
+                            o.x = f.x + a.scale * (v[4 * dy + 0] + a.bias[4 * dy + 0]);
+                            o.y = f.y + a.scale * (v[4 * dy + 1] + a.bias[4 * dy + 1]);
+                            o.z = f.z + a.scale * (v[4 * dy + 2] + a.bias[4 * dy + 2]);
+                            o.w = f.w + a.scale * (v[4 * dy + 3] + a.bias[4 * dy + 3]);
+                            *reinterpret_cast<float4 *>(a.img + base + (size_t)dy * W4) = o;
+                        }
+                    }
+                    continue;
+                }
+                for (int c = 0; c < Cout; c += 8) {
+                    float v[8];
+                    ld8(tbase + (uint32_t)c, v);
+                    if (!inside) continue;
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        v[j] += a.bias[c + j];
+                        if (a.relu) v[j] = fmaxf(v[j], 0.f);
+                    }
+                    const int g = c >> 3;
+                    if (a.mode == EPI_STORE) {
+                        bf16 *dst = a.out + ((size_t)g * a.gi.alloc + a.gi.guard + q) * 8;
+                        *reinterpret_cast<uint4 *>(dst) = pack8(v);
+                    } else {
+                        // nearest 2x up-sampling plus the skip tensor, at the output grid; the
+                        // decoder activation is rounded to BF16 first, as where it is stored
+#pragma unroll
+                        for (int j = 0; j < 8; j++) v[j] = __bfloat162float(__float2bfloat16(v[j]));
+                        const int Wo = a.go.W + 2, Ho = a.go.H + 2;
+#pragma unroll
+                        for (int i = 0; i < 2; i++)
+#pragma unroll
+                            for (int j = 0; j < 2; j++) {
+                                const long long qo = ((long long)b * Ho + 2 * y + i + 1) * Wo + 2 * x + j + 1;
+                                const size_t off = ((size_t)g * a.go.alloc + a.go.guard + qo) * 8;
+                                float w[8];
+#pragma unroll
+                                for (int k = 0; k < 8; k++) w[k] = v[k];
+                                unpack8_add(*reinterpret_cast<const uint4 *>(a.skip + off), w);
+                                *reinterpret_cast<uint4 *>(a.out + off) = pack8(w);
+                            }
+                    }
+                }
+            }
+            fence_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&t_empty[ab]);
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ small CG kernels
+
+#define CG_LOOP(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// fbp [B][4H][4W] -> CG x0 (16 channels, two planes): channel 4*dy + dx = fbp[4y+dy][4x+dx] / s
+__global__ void k_cg_unshuffle(const float *__restrict__ fbp, bf16 *__restrict__ x0, CGGeom g, float inv_s)
+{
+    const long long n = (long long)g.B * g.H * g.W;
+    CG_LOOP(i, n) {
+        const int x = (int)(i % g.W), y = (int)((i / g.W) % g.H);
+        const long long b = i / ((long long)g.W * g.H);
+        const size_t W4 = (size_t)4 * g.W;
+        const float *src = fbp + ((size_t)b * 4 * g.H + 4 * y) * W4 + 4 * x;
+        float v[16];
+#pragma unroll
+        for (int dy = 0; dy < 4; dy++) {
+            const float4 f = *reinterpret_cast<const float4 *>(src + dy * W4);
+            v[4 * dy] = f.x * inv_s;
+            v[4 * dy + 1] = f.y * inv_s;
+            v[4 * dy + 2] = f.z * inv_s;
+            v[4 * dy + 3] = f.w * inv_s;
+        }
+        const long long q = (b * (g.H + 2) + y + 1) * (g.W + 2) + x + 1;
+        float lo[8], hi[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            lo[k] = v[k];
+            hi[k] = v[8 + k];
+        }
+        *reinterpret_cast<uint4 *>(x0 + ((size_t)g.guard + q) * 8) = pack8(lo);
+        *reinterpret_cast<uint4 *>(x0 + ((size_t)g.alloc + g.guard + q) * 8) = pack8(hi);
+    }
+}
+
+// 2x2 average pool between CG tensors (gi -> go = gi / 2), C/8 planes
+__global__ void k_cg_pool(const bf16 *__restrict__ in, bf16 *__restrict__ out, CGGeom gi, CGGeom go, int planes)
+{
+    const long long n = (long long)planes * go.B * go.H * go.W;
+    CG_LOOP(i, n) {
+        const int x = (int)(i % go.W), y = (int)((i / go.W) % go.H);
+        const long long r = i / ((long long)go.W * go.H);
+        const int b = (int)(r % go.B), p = (int)(r / go.B);
+        const long long qi = ((long long)b * (gi.H + 2) + 2 * y + 1) * (gi.W + 2) + 2 * x + 1;
+        const bf16 *s = in + ((size_t)p * gi.alloc + gi.guard + qi) * 8;
+        float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        unpack8_add(*reinterpret_cast<const uint4 *>(s), v);
+        unpack8_add(*reinterpret_cast<const uint4 *>(s + 8), v);
+        unpack8_add(*reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 2) * 8), v);
+        unpack8_add(*reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 3) * 8), v);
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] *= 0.25f;
+        const long long qo = ((long long)b * (go.H + 2) + y + 1) * (go.W + 2) + x + 1;
+        *reinterpret_cast<uint4 *>(out + ((size_t)p * go.alloc + go.guard + qo) * 8) = pack8(v);
+    }
+}
+
+// [Cout][9][Cin] FP32 master weights -> [9][Cin/8][Cout][8] BF16 (K-major tiles per tap)
+__global__ void k_cg_arrange(const float *__restrict__ w, bf16 *__restrict__ wt, int Cout, int Cin)
+{
+    const long long n = (long long)Cout * 9 * Cin;
+    CG_LOOP(i, n) {
+        const int ci = (int)(i % Cin), t = (int)((i / Cin) % 9), co = (int)(i / (9LL * Cin));
+        wt[(((size_t)t * (Cin / 8) + ci / 8) * Cout + co) * 8 + (ci & 7)] = __float2bfloat16(w[i]);
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+static CGGeom cg_geom(int B, int H, int W, int max_tile_rows)
+{
+    CGGeom g;
+    g.B = B;
+    g.H = H;
+    g.W = W;
+    g.rows = (long long)B * (H + 2) * (W + 2);
+    g.guard = (W + 3 + 7) / 8 * 8;
+    // tail: the last tile may extend max_tile_rows past the end, plus its halo
+    g.alloc = g.guard + g.rows + max_tile_rows + W + 3 + 8;
+    return g;
+}
+
+struct CGBuf {
+    DevBuf buf;
+    CGGeom g;
+    int C = 0;
+    bf16 *ptr() const { return buf.as<bf16>(); }
+};
+
+static ufob_status cg_alloc(CGBuf &t, int B, int H, int W, int C, cudaStream_t s)
+{
+    const CGGeom g = cg_geom(B, H, W, 4 * 128);
+    const size_t bytes = (size_t)(C / 8) * g.alloc * 16;
+    const bool same = t.C == C && t.g.B == B && t.g.H == H && t.g.W == W && t.buf.ptr;
+    if (!same) {
+        UFOB_TRY(t.buf.ensure(bytes));
+        UFOB_CUDA_TRY(cudaMemsetAsync(t.buf.ptr, 0, bytes, s));  // border, guard and tail rows stay zero
+        t.g = g;
+        t.C = C;
+    }
+    return UFOB_OK;
+}
+
+struct FastNet {
+    DevBuf wt[8];
+    CGBuf x0, e1, p1, e2, p2, e3, p3, e4, u3, u2, u1;
+    int smem_attr = 0;
+};
+
+static int pick_mt(int Cout)
+{
+    int mt = 512 / (2 * Cout);  // two accumulator buffers in 512 TMEM columns
+    return std::max(1, std::min(4, mt));
+}
+
+static size_t conv_smem(int Cin, int Cout, int W, int MT)
+{
+    const int cgc = Cin < 64 ? Cin / 8 : 8;
+    const size_t arows = (size_t)MT * 128 + 2 * (W + 3);
+    return (size_t)kAStages * arows * 16 * cgc + (size_t)kBStages * cgc * Cout * 16 + 1024;
+}
+
+static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const float *bias, int Cout, int relu,
+                           int mode, CGBuf *out, const CGBuf *skip, const float *fbp, float *img, float scale,
+                           cudaStream_t s)
+{
+    FastConvArgs a{};
+    a.in = in.ptr();
+    a.wt = wt;
+    a.bias = bias;
+    a.gi = in.g;
+    a.Cin = in.C;
+    a.Cout = Cout;
+    a.relu = relu;
+    a.mode = mode;
+    a.MT = pick_mt(Cout);
+    a.err = device_error_word();
+    a.scale = scale;
+    if (mode == EPI_STORE) a.out = out->ptr();
+    if (mode == EPI_UPADD) {
+        a.out = out->ptr();
+        a.skip = skip->ptr();
+        a.go = out->g;
+    }
+    a.fbp = fbp;
+    a.img = img;
+    a.ntiles = (in.g.rows + a.MT * 128 - 1) / (a.MT * 128);
+    const size_t smem = conv_smem(in.C, Cout, in.g.W, a.MT);
+    if (smem > kMaxSmem) return fail(UFOB_ERR_UNSUPPORTED, "cnn: convolution tile does not fit in shared memory");
+    if (!f->smem_attr) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_conv_cg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+        f->smem_attr = 1;
+    }
+    // one CTA per SM: the two accumulator buffers may take all 512 TMEM columns
+    const long long grid = std::min<long long>(a.ntiles, num_sms());
+    k_conv_cg<<<(unsigned)grid, kThreads, std::max<size_t>(smem, 116 * 1024), s>>>(a);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, (long long)num_sms() * 16); }
+
+void *cnn_fast_create() { return new FastNet; }
+void cnn_fast_destroy(void *p) { delete static_cast<FastNet *>(p); }
+
+// Re-arrange the FP32 master weights of the 8 layers into the per-tap BF16 tiles.
+ufob_status cnn_fast_weights(void *fp, const float *const *w, const int (*shape)[2], cudaStream_t s)
+{
+    FastNet *f = static_cast<FastNet *>(fp);
+    for (int i = 0; i < 8; i++) {
+        const int cin = shape[i][0], cout = shape[i][1];
+        const size_t n = (size_t)cout * 9 * cin;
+        UFOB_TRY(f->wt[i].ensure(n * 2));
+        k_cg_arrange<<<grid_for((long long)n), 256, 0, s>>>(w[i], f->wt[i].as<bf16>(), cout, cin);
+        UFOB_CUDA_TRY(cudaGetLastError());
+        note_launch();
+    }
+    return UFOB_OK;
+}
+
+// Whole network on B slices [B][4H][4W] (H, W = quarter-resolution sides).
+ufob_status cnn_fast_forward(void *fp, const float *const *bias, const float *fbp, float *out, int B, int H, int W,
+                             float scale, cudaStream_t s)
+{
+    FastNet *f = static_cast<FastNet *>(fp);
+    UFOB_TRY(cg_alloc(f->x0, B, H, W, 16, s));
+    UFOB_TRY(cg_alloc(f->e1, B, H, W, 32, s));
+    UFOB_TRY(cg_alloc(f->p1, B, H / 2, W / 2, 32, s));
+    UFOB_TRY(cg_alloc(f->e2, B, H / 2, W / 2, 64, s));
+    UFOB_TRY(cg_alloc(f->p2, B, H / 4, W / 4, 64, s));
+    UFOB_TRY(cg_alloc(f->e3, B, H / 4, W / 4, 128, s));
+    UFOB_TRY(cg_alloc(f->p3, B, H / 8, W / 8, 128, s));
+    UFOB_TRY(cg_alloc(f->e4, B, H / 8, W / 8, 256, s));
+    UFOB_TRY(cg_alloc(f->u3, B, H / 4, W / 4, 128, s));
+    UFOB_TRY(cg_alloc(f->u2, B, H / 2, W / 2, 64, s));
+    UFOB_TRY(cg_alloc(f->u1, B, H, W, 32, s));
+    const long long npx = (long long)B * H * W;
+    k_cg_unshuffle<<<grid_for(npx), 256, 0, s>>>(fbp, f->x0.ptr(), f->x0.g, 1.f / scale);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    auto wt = [&](int i) { return f->wt[i].as<bf16>(); };
+    UFOB_TRY(conv_cg(f, f->x0, wt(0), bias[0], 32, 1, EPI_STORE, &f->e1, nullptr, nullptr, nullptr, 0.f, s));
+    k_cg_pool<<<grid_for(npx / 4 * 4), 256, 0, s>>>(f->e1.ptr(), f->p1.ptr(), f->e1.g, f->p1.g, 4);
+    note_launch();
+    UFOB_TRY(conv_cg(f, f->p1, wt(1), bias[1], 64, 1, EPI_STORE, &f->e2, nullptr, nullptr, nullptr, 0.f, s));
+    k_cg_pool<<<grid_for(npx / 16 * 8), 256, 0, s>>>(f->e2.ptr(), f->p2.ptr(), f->e2.g, f->p2.g, 8);
+    note_launch();
+    UFOB_TRY(conv_cg(f, f->p2, wt(2), bias[2], 128, 1, EPI_STORE, &f->e3, nullptr, nullptr, nullptr, 0.f, s));
+    k_cg_pool<<<grid_for(npx / 64 * 16), 256, 0, s>>>(f->e3.ptr(), f->p3.ptr(), f->e3.g, f->p3.g, 16);
+    note_launch();
+    UFOB_TRY(conv_cg(f, f->p3, wt(3), bias[3], 256, 1, EPI_STORE, &f->e4, nullptr, nullptr, nullptr, 0.f, s));
+    UFOB_TRY(conv_cg(f, f->e4, wt(4), bias[4], 128, 1, EPI_UPADD, &f->u3, &f->e3, nullptr, nullptr, 0.f, s));
+    UFOB_TRY(conv_cg(f, f->u3, wt(5), bias[5], 64, 1, EPI_UPADD, &f->u2, &f->e2, nullptr, nullptr, 0.f, s));
+    UFOB_TRY(conv_cg(f, f->u2, wt(6), bias[6], 32, 1, EPI_UPADD, &f->u1, &f->e1, nullptr, nullptr, 0.f, s));
+    UFOB_TRY(conv_cg(f, f->u1, wt(7), bias[7], 16, 0, EPI_FINAL, nullptr, nullptr, fbp, out, scale, s));
+    UFOB_CUDA_TRY(cudaGetLastError());
+    return UFOB_OK;
+}
+
+}  // namespace ufob

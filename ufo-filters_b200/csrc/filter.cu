@@ -261,7 +261,7 @@ __device__ float2 *fft_smem(float2 *a, float2 *b, const float2 *tw, uint32_t N, 
     return a;
 }
 
-enum OutKind { OUT_F32 = 0, OUT_F16 = 1, OUT_BF16 = 2, OUT_F16_PAIRS = 3, OUT_BF16_PAIRS = 4 };
+enum OutKind { OUT_F32 = 0, OUT_F16 = 1, OUT_BF16 = 2, OUT_F16_PAIRS = 3, OUT_BF16_PAIRS = 4, OUT_F16_QUADS = 5 };
 
 template <int OUT>
 __device__ __forceinline__ void store_value(void *out, size_t idx, float v)
@@ -274,7 +274,7 @@ __device__ __forceinline__ void store_value(void *out, size_t idx, float v)
 template <int OUT>
 __device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
 {
-    if (OUT == OUT_F16_PAIRS) {
+    if (OUT == OUT_F16_PAIRS || OUT == OUT_F16_QUADS) {
         __half2 h = __floats2half2_rn(lo, hi);
         return *reinterpret_cast<uint32_t *>(&h);
     } else {
@@ -283,14 +283,29 @@ __device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
     }
 }
 
-// Filter rows 2*pair and 2*pair+1 (one complex FFT of a + i b) in shared memory.
+// Filter two rows (one complex FFT of a + i b) in shared memory: rows 2*pair
+// and 2*pair+1, or for the slice-quad layout (OUT_F16_QUADS, `P` angles per
+// slice) item pair = (group * P + angle) * 2 + half, i.e. slices
+// 4*group + 2*half and 4*group + 2*half + 1 at one angle.
 template <int OUT>
 __device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32_t width, uint32_t rows,
                                             uint32_t in_pitch, uint32_t pair, float2 *bufA, float2 *bufB,
                                             const float2 *tw, const float2 *gains, uint32_t N, int log2N,
-                                            void *__restrict__ out, uint32_t out_w, uint32_t out_pitch)
+                                            void *__restrict__ out, uint32_t out_w, uint32_t out_pitch,
+                                            uint32_t P = 0)
 {
-    const uint32_t ra = 2 * pair, rb = 2 * pair + 1;
+    uint32_t ra = 2 * pair, rb = 2 * pair + 1, half = 0;
+    size_t cell0 = 0;
+    bool hasa = true;
+    if (OUT == OUT_F16_QUADS) {
+        const uint32_t gp = pair >> 1;  // group * P + angle
+        half = pair & 1u;
+        const uint32_t grp = gp / P, ang = gp - grp * P;
+        ra = (4 * grp + 2 * half) * P + ang;
+        rb = ra + P;
+        hasa = ra < rows;
+        cell0 = (size_t)gp * out_pitch;
+    }
     const bool hasb = rb < rows;
     const float *pa = in + (size_t)ra * in_pitch;
     const float *pb = in + (size_t)rb * in_pitch;
@@ -298,7 +313,7 @@ __device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32
     for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
         float a = 0.f, b = 0.f;
         if (n < width) {
-            a = __ldg(pa + n);
+            if (hasa) a = __ldg(pa + n);
             if (hasb) b = __ldg(pb + n);
         }
         bufA[n] = make_float2(a, b);
@@ -318,7 +333,18 @@ __device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32
     __syncthreads();
     float2 *other = (Z == bufA) ? bufB : bufA;
     float2 *X = fft_smem<true>(Z, other, tw, N, log2N);
-    if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
+    if (OUT == OUT_F16_QUADS) {
+        // words `half` (taps j-1) and 2 + `half` (taps j) of cell j; rows a, b in the low, high halves
+        uint32_t *o = reinterpret_cast<uint32_t *>(out) + cell0 * 4;
+        for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
+            float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
+            float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
+            if (!hasa) lo.x = hi.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
+            if (!hasb) lo.y = hi.y = 0.f;
+            o[(size_t)j * 4 + half] = pack_pair<OUT>(lo.x, lo.y);
+            o[(size_t)j * 4 + 2 + half] = pack_pair<OUT>(hi.x, hi.y);
+        }
+    } else if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
         uint32_t *o = reinterpret_cast<uint32_t *>(out);
         for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
             float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
@@ -341,7 +367,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__r
                                                                 const float2 *__restrict__ g_tw,
                                                                 const float2 *__restrict__ g_gains, uint32_t N,
                                                                 int log2N, void *__restrict__ out, uint32_t out_w,
-                                                                uint32_t out_pitch)
+                                                                uint32_t out_pitch, uint32_t npairs, uint32_t P)
 {
     extern __shared__ float4 smem_f4[];
     float2 *bufA = reinterpret_cast<float2 *>(smem_f4);
@@ -352,9 +378,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__r
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) tw[i] = g_tw[i];
     for (uint32_t i = threadIdx.x; i <= N / 2; i += blockDim.x) gains[i] = g_gains[i];
 
-    const uint32_t npairs = (rows + 1) / 2;
     for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x)
-        filter_pair<OUT>(in, width, rows, in_pitch, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch);
+        filter_pair<OUT>(in, width, rows, in_pitch, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch, P);
 }
 
 // Persistent filter stage of an uneven batch: work items (job, row pair) are
@@ -392,7 +417,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_batch(const BatchFilt
 
 template <int OUT>
 static ufob_status launch_rows(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
-                               uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s)
+                               uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s,
+                               uint32_t P = 0)
 {
     const uint32_t N = plan.nfft;
     const size_t smem = sizeof(float2) * (3 * (size_t)N + N / 2 + 1);
@@ -406,13 +432,14 @@ static ufob_status launch_rows(const FilterPlan &plan, const float *d_in, uint32
     int per_sm = 0;
     UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_rows<OUT>, kFilterThreads, smem));
     if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);
-    const uint32_t npairs = (rows + 1) / 2;
+    // slice-quad layout: two items per (group of four slices, angle)
+    const uint32_t npairs = OUT == OUT_F16_QUADS ? (rows / P + 3) / 4 * P * 2 : (rows + 1) / 2;
     uint32_t grid = (uint32_t)num_sms() * (uint32_t)per_sm * 4;
     if (grid > npairs) grid = npairs;
     if (grid == 0) return UFOB_OK;
     k_filter_rows<OUT><<<grid, kFilterThreads, smem, s>>>(d_in, width, rows, in_pitch, plan.d_twiddle.as<float2>(),
                                                           plan.d_gains.as<float2>(), N, log2N, d_out, out_w,
-                                                          out_pitch);
+                                                          out_pitch, npairs, P);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
@@ -441,6 +468,21 @@ ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32
     case UFOB_BF16: return launch_rows<OUT_BF16>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
     default: return fail(UFOB_ERR_INVALID, "filter: unsupported output dtype %d", (int)out_dtype);
     }
+}
+
+// Filter a stack of `nz` sinograms of P rows into the slice-quad FP16 layout
+// ([ceil(nz/4)][P][out_pitch] cells of 16 bytes; see backproject.cu).
+ufob_status filter_quads_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t P, uint32_t nz,
+                                uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch,
+                                cudaStream_t stream)
+{
+    const uint32_t N = plan.nfft;
+    if (N > kMaxFusedFFT || N < 4)
+        return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u outside the supported range [4, %u]", N, kMaxFusedFFT);
+    if (width > N || out_w > N || in_pitch < width || out_pitch < out_w + 1 || !P)
+        return fail(UFOB_ERR_INVALID, "filter: bad slice-quad sizes (width %u, N %u, crop %u, pitch %u)", width, N,
+                    out_w, out_pitch);
+    return launch_rows<OUT_F16_QUADS>(plan, d_in, width, P * nz, in_pitch, d_out, out_w, out_pitch, stream, P);
 }
 
 // The reference `filter` kernel alone (filter.cl:20-29): out[y][x] = in[y][x] * coeff[x].

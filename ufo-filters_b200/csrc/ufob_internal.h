@@ -99,6 +99,16 @@ enum SinoKind { SINO_F32 = 0, SINO_F16_PAIRS = 1, SINO_BF16_PAIRS = 2 };
 ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
                              uint64_t slice_pitch, float *d_out, bool kahan, int tile, cudaStream_t stream);
 
+// Slice-quad FP16 form (four slices' tap pairs per 16-byte cell): filter stage
+// and backprojection.  acc: 0 FP32 accumulation of every product, 1 FP16 lerp
+// + FP32 accumulation, 2 FP16 sums over 8-angle blocks + FP32 accumulation.
+ufob_status filter_quads_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t P, uint32_t nz,
+                                uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch,
+                                cudaStream_t stream);
+ufob_status bp_quads_launch(const BPGeometry &g, const void *d_sino, uint32_t pitch, uint64_t group_pitch,
+                            float *d_out, bool kahan, int acc, int tile, cudaStream_t stream);
+int bp_quad_tiles();
+
 // Kernel arguments of one backprojection (one stack or one batch job).
 struct BPArgs {
     uint32_t P, nz;

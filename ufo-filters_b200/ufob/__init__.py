@@ -15,14 +15,14 @@ import math
 import os
 
 __all__ = ["lib", "UfobError", "get_task", "FilterTask", "BackprojectTask", "FBP", "GeneralBackprojectTask",
-           "Batch", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS"]
+           "Batch", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libufob.so")
 
 OK, ERR_INVALID, ERR_SETUP, ERR_REQUISITION, ERR_CUDA, ERR_NOMEM, ERR_TIMEOUT, ERR_UNSUPPORTED = range(8)
 F32, F16, BF16, F64, U8, U16, U32 = range(7)
-ROWS, PAIRS = 0, 1
+ROWS, PAIRS, QUADS = 0, 1, 2
 FILTERS = ["ramp", "ramp-fromreal", "butterworth", "faris-byer", "hamming", "bh3"]
 DTYPES = {"f32": F32, "float": F32, "f16": F16, "half": F16, "bf16": BF16, "f64": F64, "double": F64,
           "u8": U8, "uchar": U8, "u16": U16, "ushort": U16, "u32": U32, "uint": U32}
@@ -46,7 +46,8 @@ class BPProps(ctypes.Structure):
     _fields_ = [("num_projections", ctypes.c_uint32), ("offset", ctypes.c_uint32), ("axis_pos", ctypes.c_double),
                 ("angle_step", ctypes.c_double), ("angle_offset", ctypes.c_double), ("mode", ctypes.c_int),
                 ("roi_x", ctypes.c_uint32), ("roi_y", ctypes.c_uint32), ("roi_width", ctypes.c_uint32),
-                ("roi_height", ctypes.c_uint32), ("compensated", ctypes.c_int), ("tile", ctypes.c_int)]
+                ("roi_height", ctypes.c_uint32), ("compensated", ctypes.c_int), ("tile", ctypes.c_int),
+                ("half_sums", ctypes.c_int)]
 
 
 class Job(ctypes.Structure):
@@ -76,6 +77,7 @@ def lib():
             "ufob_filter_set_property_string": ([vp, cs, cs], i),
             "ufob_filter_get_requisition": ([vp, u32, u32, pu32, pu32], i),
             "ufob_filter_run": ([vp, vp, u32, u32, u32, vp, i, i, u32, vp], i),
+            "ufob_filter_run_quads": ([vp, vp, u32, u32, u32, u32, vp, u32, vp], i),
             "ufob_filter_coefficients": ([vp, u32, vp, u32], i),
             "ufob_filter_apply_spectrum": ([vp, vp, vp, u32, u32, vp], i),
             "ufob_filter_destroy": ([vp], None),
@@ -114,6 +116,18 @@ def lib():
             "ufob_forwardproject": ([vp, u32, u32, d, d, vp, vp], i),
             "ufob_phantom_images": ([vp, vp, u32, u32, d, d, i, vp, vp], i),
             "ufob_measure_peaks": ([ctypes.POINTER(d), ctypes.POINTER(d)], i),
+            "ufob_cnn_create": ([u64, ctypes.c_float, ctypes.POINTER(vp)], i),
+            "ufob_cnn_destroy": ([vp], None),
+            "ufob_cnn_forward": ([vp, vp, vp, i, i, i, vp], i),
+            "ufob_cnn_forward_nhwc": ([vp, vp, vp, i, i, i, vp], i),
+            "ufob_cnn_train_step": ([vp, vp, vp, i, i, i, ctypes.c_float, ctypes.POINTER(d), vp], i),
+            "ufob_cnn_num_params": ([], u64),
+            "ufob_cnn_get_state": ([vp, i, vp, u64], i),
+            "ufob_cnn_set_state": ([vp, i, vp, u64], i),
+            "ufob_cnn_get_step": ([vp], ctypes.c_int64),
+            "ufob_cnn_set_step": ([vp, ctypes.c_int64], i),
+            "ufob_conv3x3_forward": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
+            "ufob_conv3x3_wgrad": ([vp, vp, vp, i, i, i, i, i, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -219,7 +233,8 @@ class FilterTask(_Task):
 
     def process(self, sino, dtype=F32, layout=ROWS, out=None, stream=None):
         """Filter the rows of a float32 CUDA tensor [..., H, W]; returns [..., H, crop]
-        (or [..., H, pair_pitch] int32 pairs for layout=PAIRS)."""
+        (or [..., H, pair_pitch] int32 pairs for layout=PAIRS, or for a stack
+        [Z, H, W] with layout=QUADS the [ceil(Z/4), H, crop+1, 4] int32 slice-quad cells)."""
         import torch
         if sino.dtype != torch.float32 or not sino.is_cuda:
             raise ValueError("sinogram must be a float32 CUDA tensor")
@@ -228,6 +243,15 @@ class FilterTask(_Task):
         rows = sino.numel() // W
         cw, _ = self.get_requisition(W, 1)
         dt = DTYPES.get(dtype, dtype) if isinstance(dtype, str) else dtype
+        if layout == QUADS:
+            if dt != F16:
+                raise ValueError("the QUADS layout is F16 only")
+            s3 = sino if sino.dim() == 3 else sino.reshape(-1, *sino.shape[-2:])
+            Z, H = s3.shape[0], s3.shape[1]
+            shape = ((Z + 3) // 4, H, cw + 1, 4)
+            out = torch.empty(shape, dtype=torch.int32, device=sino.device) if out is None else out
+            check(lib().ufob_filter_run_quads(self._h, _ptr(s3), W, H, Z, W, _ptr(out), cw + 1, _stream(stream)))
+            return out
         if layout == PAIRS:
             pitch = (cw + 1 + 3) // 4 * 4
             shape = tuple(sino.shape[:-1]) + (pitch,)
@@ -275,10 +299,22 @@ class BackprojectTask(_Task):
         check(lib().ufob_backproject_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h)))
         return w.value, h.value
 
-    def process(self, sino, dtype=F32, layout=ROWS, width=None, out=None, stream=None):
+    def process(self, sino, dtype=F32, layout=ROWS, width=None, out=None, stream=None, nslices=None):
         """Backproject [H, W] or [Z, H, W] float32 sinograms (or F16/BF16 pairs
         from FilterTask.process(layout=PAIRS), then pass ``width``)."""
         import torch
+        if layout == QUADS:
+            # [G, H, cells, 4] cells from FilterTask.process(layout=QUADS); pass width and nslices
+            q = sino.contiguous()
+            G, H, cells = q.shape[0], q.shape[1], q.shape[2]
+            if width is None:
+                raise ValueError("pass width= for the QUADS layout")
+            Z = nslices or 4 * G
+            ow, oh = self.get_requisition(width, H)
+            out = torch.empty((Z, oh, ow), dtype=torch.float32, device=q.device) if out is None else out
+            check(lib().ufob_backproject_run(self._h, _ptr(q), F16, QUADS, width, H, Z, cells, cells * H, _ptr(out),
+                                             _stream(stream)))
+            return out
         squeeze = sino.dim() == 2
         s3 = sino.unsqueeze(0) if squeeze else sino
         s3 = s3.contiguous()
@@ -318,6 +354,7 @@ class FBP:
         check(L.ufob_fbp_create(ctypes.byref(fp), ctypes.byref(bpp), DTYPES.get(storage, storage)
                                 if isinstance(storage, str) else storage, ctypes.byref(h)))
         self._h = h
+        self._destroy = L.ufob_fbp_destroy
 
     def get_requisition(self, width, height):
         w, h = ctypes.c_uint32(), ctypes.c_uint32()
@@ -356,8 +393,10 @@ class FBP:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().ufob_fbp_destroy(self._h)
+        # the destroy function is bound at creation: module globals may be gone at interpreter exit
+        h, fn = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and fn:
+            fn(h)
             self._h = None
 
 
@@ -419,6 +458,7 @@ class Batch:
         h = ctypes.c_void_p()
         check(L.ufob_batch_create(ctypes.byref(fp), storage, ctypes.byref(h)))
         self._h = h
+        self._destroy = L.ufob_batch_destroy
 
     def run(self, jobs, stream=None):
         arr = (Job * len(jobs))()
@@ -431,8 +471,9 @@ class Batch:
         return int(lib().ufob_batch_variant(self._h))
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().ufob_batch_destroy(self._h)
+        h, fn = getattr(self, "_h", None), getattr(self, "_destroy", None)
+        if h and fn:
+            fn(h)
             self._h = None
 
 
