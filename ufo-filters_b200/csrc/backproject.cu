@@ -988,7 +988,8 @@ ufob_status bp_quads_launch(const BPGeometry &g, const void *d_sino, uint32_t pi
     if ((uintptr_t)d_sino & 15) return fail(UFOB_ERR_INVALID, "backproject: slice-quad base must be 16-byte aligned");
     if (pitch < g.W + 1 || group_pitch < (uint64_t)pitch * g.P)
         return fail(UFOB_ERR_INVALID, "backproject: slice-quad pitches too small");
-    if (tile < 0) tile = g.nz <= 4 ? 0 : 2;
+    // measured on B200 (2048^2 x 1500, 32 slices): 32x16 px x 16 slices, 2 stages of 16 angles is fastest
+    if (tile < 0) tile = g.nz <= 4 ? 0 : (g.nz <= 8 ? 2 : 8);
     switch (acc) {
     case QACC_F32:
         return kahan ? quads_tile<QACC_F32, true>(tile, g, d_sino, pitch, group_pitch, d_out, stream)

@@ -14,11 +14,13 @@
 // (cp.async.bulk) of one plane's row range, and the weights, pre-arranged as
 // [tap][channel group][Cout][8], are one contiguous bulk copy per tap.
 //
-// CTA roles (192 threads): warp 0 lane 0 issues the bulk copies into an
-// A ring (halo blocks, 2 stages) and a B ring (per-tap weights, 4 stages);
+// CTA roles (320 threads): warp 0 lane 0 issues the bulk copies into an
+// A ring (halo blocks, 2 stages) and a B ring of per-tap weight tiles (as deep
+// as shared memory allows; small layers keep all nine taps resident);
 // warp 1 allocates tensor memory and lane 0 issues tcgen05.mma (M = 128 rows
 // per MMA, MT row blocks per tile, N = Cout, K = 16) and tcgen05.commit;
-// warps 2-5 drain the double-buffered accumulators (tcgen05.ld) and run the
+// warps 2-9 (two per TMEM lane quarter, one channel half each) drain the
+// double-buffered accumulators (tcgen05.ld, up to 32 columns per load) and run the
 // fused epilogue: bias + ReLU + BF16 store, or the decoder's nearest 2x
 // up-sampling plus skip connection, or the output depth-to-space plus the
 // residual FBP image.  Border rows of the padded grid are never written, so
@@ -36,11 +38,12 @@ typedef __nv_bfloat16 bf16;
 
 namespace {
 
-constexpr int kThreads = 192;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;  // producer warp, MMA warp, epilogue warps
 constexpr int kAStages = 2;
-constexpr int kBStages = 4;
+constexpr int kMaxBStages = 16;
 constexpr int kErrFastTimeout = 0x2101;
-constexpr size_t kMaxSmem = 200 * 1024;
+constexpr size_t kMaxSmem = 220 * 1024;
 constexpr uint64_t kLimitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t sa(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -127,16 +130,47 @@ __device__ __forceinline__ void commit(uint64_t *b)
                  : "memory");
 }
 
-__device__ __forceinline__ void ld8(uint32_t taddr, float (&v)[8])
+// tcgen05.ld of N consecutive 32-bit columns (32 lanes x 32 bit), no wait
+template <int N>
+__device__ __forceinline__ void tld(uint32_t taddr, float (&v)[N]);
+
+template <>
+__device__ __forceinline__ void tld<8>(uint32_t taddr, float (&v)[8])
 {
-    uint32_t r[8];
+    uint32_t *r = reinterpret_cast<uint32_t *>(v);
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
+
+template <>
+__device__ __forceinline__ void tld<16>(uint32_t taddr, float (&v)[16])
+{
+    uint32_t *r = reinterpret_cast<uint32_t *>(v);
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+}
+
+template <>
+__device__ __forceinline__ void tld<32>(uint32_t taddr, float (&v)[32])
+{
+    uint32_t *r = reinterpret_cast<uint32_t *>(v);
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                 "[%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void tld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -184,6 +218,7 @@ struct FastConvArgs {
     float scale;
     CGGeom gi, go;
     int Cin, Cout, MT, relu, mode;
+    int bstages;   // weight ring depth; == 9 * chunks: all weights resident, loaded once
     long long ntiles;
     int *err;
 };
@@ -191,15 +226,18 @@ struct FastConvArgs {
 __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t a_full[kAStages], a_empty[kAStages], b_full[kBStages], b_empty[kBStages];
+    __shared__ uint64_t a_full[kAStages], a_empty[kAStages], b_full[kMaxBStages], b_empty[kMaxBStages];
     __shared__ uint64_t t_full[2], t_empty[2];
     __shared__ uint32_t tslot;
     __shared__ int abort_flag;
+    __shared__ float s_bias[256];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int Cin = a.Cin, Cout = a.Cout, MT = a.MT;
     const int cgc = Cin < 64 ? Cin / 8 : 8;  // channel groups per K chunk
     const int nchunks = Cin / (cgc * 8);
+    const int nbs = a.bstages;
+    const bool resident = nbs == 9 * nchunks;
     const int Wp = a.gi.W + 2;
     const int halo = Wp + 1;
     const int arows = MT * 128 + 2 * halo;  // rows of one staged plane
@@ -217,17 +255,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
             bar_init(&a_full[i], 1);
             bar_init(&a_empty[i], 1);
         }
-        for (int i = 0; i < kBStages; i++) {
+        for (int i = 0; i < nbs; i++) {
             bar_init(&b_full[i], 1);
             bar_init(&b_empty[i], 1);
         }
         for (int i = 0; i < 2; i++) {
             bar_init(&t_full[i], 1);
-            bar_init(&t_empty[i], 4);
+            bar_init(&t_empty[i], kEpiWarps);
         }
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int i = threadIdx.x; i < Cout; i += blockDim.x) s_bias[i] = a.bias[i];
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa(&tslot)), "r"(ncols)
                      : "memory");
@@ -245,10 +284,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
     if (warp == 0) {
         if (lane == 0) {
             uint32_t ka = 0, kb = 0;
-            int last_a[kAStages], last_b[kBStages];  // running index of each stage's last copy
+            int last_a[kAStages], last_b[kMaxBStages];  // running index of each stage's last copy
             for (int i = 0; i < kAStages; i++) last_a[i] = -1;
-            for (int i = 0; i < kBStages; i++) last_b[i] = -1;
+            for (int i = 0; i < nbs; i++) last_b[i] = -1;
             bool ok = true;
+            if (resident && blockIdx.x < a.ntiles) {
+                // every (chunk, tap) weight tile once, kept for the whole kernel
+                for (int kc = 0; kc < nchunks; kc++)
+                    for (int t = 0; t < 9; t++) {
+                        const int sb = kc * 9 + t;
+                        bar_expect(&b_full[sb], b_stage);
+                        const bf16 *src = a.wt + ((size_t)t * (Cin / 8) + (size_t)kc * cgc) * Cout * 8;
+                        bulk_g2s(sB + (size_t)sb * b_stage, src, b_stage, &b_full[sb]);
+                        last_b[sb] = 0;
+                    }
+            }
             for (long long tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
                 const long long q0 = tile * (long long)(MT * 128);
                 for (int kc = 0; kc < nchunks && ok; kc++) {
@@ -263,9 +313,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                     }
                     last_a[s] = (int)ka;
                     ka++;
-                    for (int t = 0; t < 9 && ok; t++) {
-                        const int sb = (int)(kb % kBStages);
-                        ok = bar_wait(&b_empty[sb], ((kb / kBStages) & 1u) ^ 1u, abort_p);
+                    for (int t = 0; t < 9 && ok && !resident; t++) {
+                        const int sb = (int)(kb % nbs);
+                        ok = bar_wait(&b_empty[sb], ((kb / nbs) & 1u) ^ 1u, abort_p);
                         if (!ok) break;
                         bar_expect(&b_full[sb], b_stage);
                         const bf16 *src = a.wt + ((size_t)t * (Cin / 8) + (size_t)kc * cgc) * Cout * 8;
@@ -285,10 +335,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                                now_ns() - t0 < kLimitNs / 8) {
                         }
                 }
-                for (int s = 0; s < kBStages; s++) {
+                for (int s = 0; s < nbs; s++) {
                     const uint64_t t0 = now_ns();
                     if (last_b[s] >= 0)
-                        while (!bar_try(&b_full[s], ((uint32_t)last_b[s] / kBStages) & 1u) &&
+                        while (!bar_try(&b_full[s], ((uint32_t)last_b[s] / nbs) & 1u) &&
                                now_ns() - t0 < kLimitNs / 8) {
                         }
                 }
@@ -312,10 +362,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                     fence_after();
                     const uint32_t abase = sa(sA + (size_t)s * a_stage);
                     for (int t = 0; t < 9 && ok; t++) {
-                        const int sb = (int)(kb % kBStages);
-                        ok = bar_wait(&b_full[sb], (kb / kBStages) & 1u, abort_p);
-                        if (!ok) break;
-                        fence_after();
+                        const int sb = resident ? kc * 9 + t : (int)(kb % nbs);
+                        if (!resident || it == 0) {
+                            ok = bar_wait(&b_full[sb], resident ? 0u : (kb / nbs) & 1u, abort_p);
+                            if (!ok) break;
+                            fence_after();
+                        }
                         const uint32_t bbase = sa(sB + (size_t)sb * b_stage);
                         const int off = halo + (t / 3 - 1) * Wp + (t % 3 - 1);
                         for (int m = 0; m < MT; m++) {
@@ -328,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                                 mma(dcol + (uint32_t)(m * Cout), da, db, idesc, (kc | t | k) ? 1u : 0u);
                             }
                         }
-                        commit(&b_empty[sb]);  // frees the weight stage once these MMAs finish
+                        if (!resident) commit(&b_empty[sb]);  // frees the weight stage once these MMAs finish
                         kb++;
                     }
                     commit(&a_empty[s]);
@@ -339,11 +391,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
             if (!ok) atomicExch(a.err, kErrFastTimeout);
         }
     } else {
-        // epilogue warps 2..5: TMEM lane quarter = warp % 4
-        const int quarter = warp & 3;
+        // epilogue warps 2..9: TMEM lane quarter = warp % 4, channel half = (warp - 2) / 4
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const int ch = Cout / 2;  // channels per epilogue warp
         uint32_t it = 0;
-        const int Hp = a.gi.H + 2;
-        const long long img_rows = (long long)Hp * Wp;
+        const uint32_t Hp = (uint32_t)a.gi.H + 2;
+        const uint32_t img_rows = Hp * (uint32_t)Wp;
+        const uint32_t rows = (uint32_t)a.gi.rows;
         for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
             const uint32_t ab = it & 1u;
             if (!bar_wait(&t_full[ab], (it >> 1) & 1u, abort_p)) {
@@ -351,77 +405,90 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                 break;
             }
             fence_after();
-            const long long q0 = tile * (long long)(MT * 128);
+            const uint32_t q0 = (uint32_t)tile * (uint32_t)(MT * 128);
             for (int m = 0; m < MT; m++) {
-                const long long q = q0 + m * 128 + quarter * 32 + lane;
-                const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + ab * acc_cols + (uint32_t)(m * Cout);
-                // interior test of this padded row
-                bool inside = q < a.gi.rows;
+                const uint32_t q = q0 + (uint32_t)(m * 128 + quarter * 32 + lane);
+                const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + ab * acc_cols +
+                                       (uint32_t)(m * Cout + half * ch);
+                // interior test of this padded row (32-bit index math)
+                bool inside = q < rows;
                 int b = 0, y = 0, x = 0;
                 if (inside) {
                     b = (int)(q / img_rows);
-                    const int r = (int)(q - (long long)b * img_rows);
-                    y = r / Wp - 1;
-                    x = r - (y + 1) * Wp - 1;
+                    const uint32_t r = q - (uint32_t)b * img_rows;
+                    const int yy = (int)(r / (uint32_t)Wp);
+                    y = yy - 1;
+                    x = (int)r - yy * Wp - 1;
                     inside = y >= 0 && y < a.gi.H && x >= 0 && x < a.gi.W;
                 }
                 if (a.mode == EPI_FINAL) {
-                    // Cout = 16 = 4 x 4 sub-pixels: out = fbp + s * (acc + bias)
-                    float v[16];
-                    float t8[8];
-                    ld8(tbase, t8);
-#pragma unroll
-                    for (int j = 0; j < 8; j++) v[j] = t8[j];
-                    ld8(tbase + 8, t8);
-#pragma unroll
-                    for (int j = 0; j < 8; j++) v[8 + j] = t8[j];
+                    // Cout = 16 = 4 x 4 sub-pixels; this warp: rows 2*half, 2*half + 1
+                    float v[8];
+                    tld<8>(tbase, v);
+                    tld_wait();
                     if (inside) {
                         const int W4 = 4 * a.gi.W;
-                        const size_t base = ((size_t)b * 4 * a.gi.H + 4 * y) * W4 + 4 * x;
+                        const size_t base = ((size_t)b * 4 * a.gi.H + 4 * y + 2 * half) * W4 + 4 * x;
 #pragma unroll
-                        for (int dy = 0; dy < 4; dy++) {
+                        for (int dy = 0; dy < 2; dy++) {
                             const float4 f = *reinterpret_cast<const float4 *>(a.fbp + base + (size_t)dy * W4);
+                            const float *bb = s_bias + 8 * half + 4 * dy;
                             float4 o;
-                            o.x = f.x + a.scale * (v[4 * dy + 0] + a.bias[4 * dy + 0]);
-                            o.y = f.y + a.scale * (v[4 * dy + 1] + a.bias[4 * dy + 1]);
-                            o.z = f.z + a.scale * (v[4 * dy + 2] + a.bias[4 * dy + 2]);
-                            o.w = f.w + a.scale * (v[4 * dy + 3] + a.bias[4 * dy + 3]);
+                            o.x = f.x + a.scale * (v[4 * dy + 0] + bb[0]);
+                            o.y = f.y + a.scale * (v[4 * dy + 1] + bb[1]);
+                            o.z = f.z + a.scale * (v[4 * dy + 2] + bb[2]);
+                            o.w = f.w + a.scale * (v[4 * dy + 3] + bb[3]);
                             *reinterpret_cast<float4 *>(a.img + base + (size_t)dy * W4) = o;
                         }
                     }
                     continue;
                 }
-                for (int c = 0; c < Cout; c += 8) {
-                    float v[8];
-                    ld8(tbase + (uint32_t)c, v);
+                for (int c0 = 0; c0 < ch; c0 += 32) {
+                    float v[32];
+                    const int n = ch - c0 < 32 ? ch - c0 : 32;  // 8, 16 or 32 columns
+                    if (n == 32)
+                        tld<32>(tbase + (uint32_t)c0, v);
+                    else if (n == 16)
+                        tld<16>(tbase + (uint32_t)c0, *reinterpret_cast<float(*)[16]>(v));
+                    else
+                        tld<8>(tbase + (uint32_t)c0, *reinterpret_cast<float(*)[8]>(v));
+                    tld_wait();
                     if (!inside) continue;
+                    const int cbase = half * ch + c0;
 #pragma unroll
-                    for (int j = 0; j < 8; j++) {
-                        v[j] += a.bias[c + j];
-                        if (a.relu) v[j] = fmaxf(v[j], 0.f);
-                    }
-                    const int g = c >> 3;
-                    if (a.mode == EPI_STORE) {
-                        bf16 *dst = a.out + ((size_t)g * a.gi.alloc + a.gi.guard + q) * 8;
-                        *reinterpret_cast<uint4 *>(dst) = pack8(v);
-                    } else {
-                        // nearest 2x up-sampling plus the skip tensor, at the output grid; the
-                        // decoder activation is rounded to BF16 first, as where it is stored
+                    for (int g8 = 0; g8 < 4; g8++) {
+                        if (g8 * 8 >= n) break;
+                        float w[8];
 #pragma unroll
-                        for (int j = 0; j < 8; j++) v[j] = __bfloat162float(__float2bfloat16(v[j]));
-                        const int Wo = a.go.W + 2, Ho = a.go.H + 2;
+                        for (int j = 0; j < 8; j++) {
+                            w[j] = v[g8 * 8 + j] + s_bias[cbase + g8 * 8 + j];
+                            if (a.relu) w[j] = fmaxf(w[j], 0.f);
+                        }
+                        const int g = (cbase >> 3) + g8;
+                        if (a.mode == EPI_STORE) {
+                            bf16 *dst = a.out + ((size_t)g * a.gi.alloc + a.gi.guard + q) * 8;
+                            *reinterpret_cast<uint4 *>(dst) = pack8(w);
+                        } else {
+                            // nearest 2x up-sampling plus the skip tensor at the output grid; the
+                            // decoder activation is rounded to BF16 first, as where it is stored
 #pragma unroll
-                        for (int i = 0; i < 2; i++)
+                            for (int j = 0; j < 8; j++) w[j] = __bfloat162float(__float2bfloat16(w[j]));
+                            const uint32_t Wo = (uint32_t)a.go.W + 2, Ho = (uint32_t)a.go.H + 2;
 #pragma unroll
-                            for (int j = 0; j < 2; j++) {
-                                const long long qo = ((long long)b * Ho + 2 * y + i + 1) * Wo + 2 * x + j + 1;
+                            for (int i = 0; i < 2; i++) {
+                                const uint32_t qo = ((uint32_t)b * Ho + 2 * y + i + 1) * Wo + 2 * x + 1;
                                 const size_t off = ((size_t)g * a.go.alloc + a.go.guard + qo) * 8;
-                                float w[8];
+                                const uint4 s0 = *reinterpret_cast<const uint4 *>(a.skip + off);
+                                const uint4 s1 = *reinterpret_cast<const uint4 *>(a.skip + off + 8);
+                                float o0[8], o1[8];
 #pragma unroll
-                                for (int k = 0; k < 8; k++) w[k] = v[k];
-                                unpack8_add(*reinterpret_cast<const uint4 *>(a.skip + off), w);
-                                *reinterpret_cast<uint4 *>(a.out + off) = pack8(w);
+                                for (int k = 0; k < 8; k++) o0[k] = o1[k] = w[k];
+                                unpack8_add(s0, o0);
+                                unpack8_add(s1, o1);
+                                *reinterpret_cast<uint4 *>(a.out + off) = pack8(o0);
+                                *reinterpret_cast<uint4 *>(a.out + off + 8) = pack8(o1);
                             }
+                        }
                     }
                 }
             }
@@ -527,7 +594,7 @@ struct CGBuf {
 
 static ufob_status cg_alloc(CGBuf &t, int B, int H, int W, int C, cudaStream_t s)
 {
-    const CGGeom g = cg_geom(B, H, W, 4 * 128);
+    const CGGeom g = cg_geom(B, H, W, 8 * 128);  // largest tile of plan_conv
     const size_t bytes = (size_t)(C / 8) * g.alloc * 16;
     const bool same = t.C == C && t.g.B == B && t.g.H == H && t.g.W == W && t.buf.ptr;
     if (!same) {
@@ -545,17 +612,43 @@ struct FastNet {
     int smem_attr = 0;
 };
 
-static int pick_mt(int Cout)
-{
-    int mt = 512 / (2 * Cout);  // two accumulator buffers in 512 TMEM columns
-    return std::max(1, std::min(4, mt));
-}
+// Tile plan of one layer: row blocks per tile (two accumulator buffers of
+// MT * Cout columns in the 512 TMEM columns), weight ring depth, smem bytes.
+struct ConvPlan {
+    int MT, bstages;
+    size_t smem;
+    long long ntiles;
+};
 
-static size_t conv_smem(int Cin, int Cout, int W, int MT)
+static ConvPlan plan_conv(int Cin, int Cout, const CGGeom &g)
 {
     const int cgc = Cin < 64 ? Cin / 8 : 8;
-    const size_t arows = (size_t)MT * 128 + 2 * (W + 3);
-    return (size_t)kAStages * arows * 16 * cgc + (size_t)kBStages * cgc * Cout * 16 + 1024;
+    const int nchunks = Cin / (cgc * 8);
+    const size_t b_stage = (size_t)cgc * Cout * 16;
+    const int sms = num_sms();
+    ConvPlan best{0, 0, 0, 0};
+    for (int mt = 8; mt >= 1; mt >>= 1) {
+        if (2 * mt * Cout > 512) continue;
+        const size_t arows = (size_t)mt * 128 + 2 * (g.W + 3);
+        const size_t abytes = (size_t)kAStages * arows * 16 * cgc + 1024;
+        if (abytes + 2 * b_stage > kMaxSmem) continue;
+        ConvPlan p;
+        p.MT = mt;
+        p.ntiles = (g.rows + mt * 128 - 1) / (mt * 128);
+        const int nres = 9 * nchunks;
+        if (nres <= kMaxBStages && abytes + nres * b_stage <= kMaxSmem)
+            p.bstages = nres;  // all weights resident
+        else
+            p.bstages = (int)std::min<size_t>(kMaxBStages, std::min<size_t>(nres - 1, (kMaxSmem - abytes) / b_stage));
+        p.smem = abytes + (size_t)p.bstages * b_stage;
+        // largest tile that still gives every SM work; else the one with most tiles
+        if (!best.MT || (best.ntiles < sms && p.ntiles > best.ntiles)) best = p;
+        if (p.ntiles >= sms) {
+            best = p;
+            break;
+        }
+    }
+    return best;
 }
 
 static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const float *bias, int Cout, int relu,
@@ -571,7 +664,12 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
     a.Cout = Cout;
     a.relu = relu;
     a.mode = mode;
-    a.MT = pick_mt(Cout);
+    if (in.g.alloc >= (1ll << 31) || (mode == EPI_UPADD && out->g.alloc >= (1ll << 31)))
+        return fail(UFOB_ERR_UNSUPPORTED, "cnn: batch too large for 32-bit row indices");
+    const ConvPlan pl = plan_conv(in.C, Cout, in.g);
+    if (!pl.MT) return fail(UFOB_ERR_UNSUPPORTED, "cnn: convolution tile does not fit in shared memory");
+    a.MT = pl.MT;
+    a.bstages = pl.bstages;
     a.err = device_error_word();
     a.scale = scale;
     if (mode == EPI_STORE) a.out = out->ptr();
@@ -582,9 +680,8 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
     }
     a.fbp = fbp;
     a.img = img;
-    a.ntiles = (in.g.rows + a.MT * 128 - 1) / (a.MT * 128);
-    const size_t smem = conv_smem(in.C, Cout, in.g.W, a.MT);
-    if (smem > kMaxSmem) return fail(UFOB_ERR_UNSUPPORTED, "cnn: convolution tile does not fit in shared memory");
+    a.ntiles = pl.ntiles;
+    const size_t smem = pl.smem;
     if (!f->smem_attr) {
         UFOB_CUDA_TRY(cudaFuncSetAttribute(k_conv_cg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
         f->smem_attr = 1;

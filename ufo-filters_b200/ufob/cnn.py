@@ -8,7 +8,8 @@ the GPU, forward-projected with the engine's projector over 90 and 1800
 angles, and reconstructed with the engine's FBP; the target is the
 1800-angle FBP.  Plain FBP stays the fallback and the judge of the error.
 
-All compute runs in libufob (cnn_net.cu, cnn_conv.cu); this module holds the
+All compute runs in libufob (cnn_net.cu, cnn_conv.cu for training, cnn_fast.cu
+for inference); this module holds the
 data generation loop, checkpointing and evaluation.
 """
 from __future__ import annotations
@@ -79,7 +80,7 @@ class SparseViewNet:
         self.n_params = int(lib().ufob_cnn_num_params())
 
     def forward(self, fbp, out=None, stream=None):
-        """[B, H, W] FP32 CUDA tensor (sides multiples of 16) -> corrected slices."""
+        """[B, H, W] FP32 CUDA tensor (sides multiples of 32) -> corrected slices."""
         import torch
         x = fbp.contiguous()
         B, H, W = x.shape
