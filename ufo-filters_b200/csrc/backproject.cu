@@ -71,14 +71,20 @@ __device__ __forceinline__ uint64_t global_timer_ns()
     return t;
 }
 
-// Wait for phase `parity` of `bar`, giving up after `limit_ns`.
+// Wait for phase `parity` of `bar`, giving up after `limit_ns`.  The timer is
+// read only every 256 polls so that its latency does not delay the wake-up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
 {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_timer_ns();
-    while (true) {
+    uint64_t t0 = 0;
+    for (uint32_t i = 1;; i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_timer_ns() - t0 > limit_ns) return false;
+        if ((i & 255u) == 0) {
+            const uint64_t t = global_timer_ns();
+            if (!t0)
+                t0 = t;
+            else if (t - t0 > limit_ns)
+                return false;
+        }
     }
 }
 

@@ -41,11 +41,12 @@ __device__ __forceinline__ void cnn_mbar_init(uint64_t *bar)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(cvta_smem(bar)) : "memory");
 }
 
+// Bounded wait (2 s); the timer is read only every 256 polls so that its
+// latency does not delay noticing the phase flip.
 __device__ __forceinline__ bool cnn_mbar_wait(uint64_t *bar, uint32_t parity)
 {
-    uint64_t t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    while (true) {
+    uint64_t t0 = 0;
+    for (uint32_t i = 1;; i++) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
@@ -53,9 +54,14 @@ __device__ __forceinline__ bool cnn_mbar_wait(uint64_t *bar, uint32_t parity)
             : "r"(cvta_smem(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
-        uint64_t t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        if (t - t0 > 2000000000ull) return false;
+        if ((i & 255u) == 0) {
+            uint64_t t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (!t0)
+                t0 = t;
+            else if (t - t0 > 2000000000ull)
+                return false;
+        }
     }
 }
 

@@ -72,18 +72,24 @@ __device__ __forceinline__ uint64_t now_ns()
 }
 
 // Bounded wait that also gives up as soon as another role raised the abort flag.
+// The timer and the flag are checked only every 256 polls: a %globaltimer read
+// per poll delays noticing the phase flip by the read's latency.
 __device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile int *abort_flag)
 {
-    if (bar_try(b, parity)) return true;
-    const uint64_t t0 = now_ns();
-    while (!bar_try(b, parity)) {
-        if (*abort_flag) return false;
-        if (now_ns() - t0 > kLimitNs) {
-            *abort_flag = 1;
-            return false;
+    uint64_t t0 = 0;
+    for (uint32_t i = 1;; i++) {
+        if (bar_try(b, parity)) return true;
+        if ((i & 255u) == 0) {
+            if (*abort_flag) return false;
+            const uint64_t t = now_ns();
+            if (!t0) {
+                t0 = t;
+            } else if (t - t0 > kLimitNs) {
+                *abort_flag = 1;
+                return false;
+            }
         }
     }
-    return true;
 }
 
 __device__ __forceinline__ void bar_arrive(uint64_t *b)
@@ -170,6 +176,8 @@ __device__ __forceinline__ void tld<32>(uint32_t taddr, float (&v)[32])
                  : "r"(taddr));
 }
 
+__device__ __forceinline__ int ilog2_dev(int v) { return 31 - __clz(v); }
+
 __device__ __forceinline__ void tld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -223,6 +231,25 @@ struct FastConvArgs {
     int *err;
 };
 
+// The MMAs of one tap, fully unrolled: MT row blocks x KS K-steps of 16
+// channels.  The descriptors of the tap are built once; each MMA adds a
+// compile-time row / channel-group offset to the 16-byte start-address field
+// (smem addresses stay below 256 KB, so the field never carries).  A single
+// thread issues every MMA, so its per-MMA instruction count bounds the
+// tensor-core rate for small N.
+template <int MT, int KS>
+__device__ __forceinline__ void issue_tap(uint32_t dcol, uint32_t Cout, uint64_t dA, uint64_t dB, uint32_t a16,
+                                          uint32_t b16, uint32_t idesc, bool first)
+{
+#pragma unroll
+    for (int m = 0; m < MT; m++)
+#pragma unroll
+        for (int k = 0; k < KS; k++)
+            mma(dcol + (uint32_t)m * Cout, dA + (uint64_t)(m * 128) + (uint64_t)(2 * k) * a16,
+                dB + (uint64_t)(2 * k) * b16, idesc, (first && k == 0) ? 0u : 1u);
+}
+
+template <int MT, int KS>
 __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -233,7 +260,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
     __shared__ float s_bias[256];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int Cin = a.Cin, Cout = a.Cout, MT = a.MT;
+    const int Cin = a.Cin, Cout = a.Cout;
     const int cgc = Cin < 64 ? Cin / 8 : 8;  // channel groups per K chunk
     const int nchunks = Cin / (cgc * 8);
     const int nbs = a.bstages;
@@ -370,16 +397,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                         }
                         const uint32_t bbase = sa(sB + (size_t)sb * b_stage);
                         const int off = halo + (t / 3 - 1) * Wp + (t % 3 - 1);
-                        for (int m = 0; m < MT; m++) {
-                            for (int k = 0; k < cgc / 2; k++) {
-                                const uint64_t da =
-                                    desc_kmajor(abase + (uint32_t)(off + m * 128) * 16 + (uint32_t)k * 2 * a_plane,
-                                                a_plane, 128);
-                                const uint64_t db =
-                                    desc_kmajor(bbase + (uint32_t)k * 2 * (uint32_t)Cout * 16, (uint32_t)Cout * 16, 128);
-                                mma(dcol + (uint32_t)(m * Cout), da, db, idesc, (kc | t | k) ? 1u : 0u);
-                            }
-                        }
+                        issue_tap<MT, KS>(dcol, (uint32_t)Cout, desc_kmajor(abase + (uint32_t)off * 16, a_plane, 128),
+                                          desc_kmajor(bbase, (uint32_t)Cout * 16, 128), a_plane >> 4, (uint32_t)Cout,
+                                          idesc, kc == 0 && t == 0);
                         if (!resident) commit(&b_empty[sb]);  // frees the weight stage once these MMAs finish
                         kb++;
                     }
@@ -405,89 +425,150 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                 break;
             }
             fence_after();
-            const uint32_t q0 = (uint32_t)tile * (uint32_t)(MT * 128);
-            for (int m = 0; m < MT; m++) {
-                const uint32_t q = q0 + (uint32_t)(m * 128 + quarter * 32 + lane);
-                const uint32_t tbase = tmem + ((uint32_t)(quarter * 32) << 16) + ab * acc_cols +
-                                       (uint32_t)(m * Cout + half * ch);
-                // interior test of this padded row (32-bit index math)
-                bool inside = q < rows;
-                int b = 0, y = 0, x = 0;
-                if (inside) {
-                    b = (int)(q / img_rows);
-                    const uint32_t r = q - (uint32_t)b * img_rows;
-                    const int yy = (int)(r / (uint32_t)Wp);
-                    y = yy - 1;
-                    x = (int)r - yy * Wp - 1;
-                    inside = y >= 0 && y < a.gi.H && x >= 0 && x < a.gi.W;
-                }
-                if (a.mode == EPI_FINAL) {
-                    // Cout = 16 = 4 x 4 sub-pixels; this warp: rows 2*half, 2*half + 1
-                    float v[8];
-                    tld<8>(tbase, v);
-                    tld_wait();
-                    if (inside) {
-                        const int W4 = 4 * a.gi.W;
-                        const size_t base = ((size_t)b * 4 * a.gi.H + 4 * y + 2 * half) * W4 + 4 * x;
+            const uint32_t q0 = (uint32_t)tile * (uint32_t)(MT * 128) + (uint32_t)(quarter * 32 + lane);
+            const uint32_t tb = tmem + ((uint32_t)(quarter * 32) << 16) + ab * acc_cols + (uint32_t)(half * ch);
+            // pixel of row q of the padded grid: (b, y, x), inside = interior pixel
+            auto locate = [&](uint32_t q, int &b, int &y, int &x) -> bool {
+                if (q >= rows) return false;
+                b = (int)(q / img_rows);
+                const uint32_t r = q - (uint32_t)b * img_rows;
+                const int yy = (int)(r / (uint32_t)Wp);
+                y = yy - 1;
+                x = (int)r - yy * Wp - 1;
+                return y >= 0 && y < a.gi.H && x >= 0 && x < a.gi.W;
+            };
+            if (a.mode == EPI_FINAL) {
+                // Cout = 16 = 4 x 4 sub-pixels; this warp: sub-rows 2*half, 2*half + 1.  The FBP loads
+                // and TMEM loads of up to 4 row blocks are in flight before each wait.
+                constexpr int MG = MT < 4 ? MT : 4;
+                const int W4 = 4 * a.gi.W;
 #pragma unroll
-                        for (int dy = 0; dy < 2; dy++) {
-                            const float4 f = *reinterpret_cast<const float4 *>(a.fbp + base + (size_t)dy * W4);
-                            const float *bb = s_bias + 8 * half + 4 * dy;
-                            float4 o;
-                            o.x = f.x + a.scale * (v[4 * dy + 0] + bb[0]);
-                            o.y = f.y + a.scale * (v[4 * dy + 1] + bb[1]);
-                            o.z = f.z + a.scale * (v[4 * dy + 2] + bb[2]);
-                            o.w = f.w + a.scale * (v[4 * dy + 3] + bb[3]);
-                            *reinterpret_cast<float4 *>(a.img + base + (size_t)dy * W4) = o;
+                for (int m0 = 0; m0 < MT; m0 += MG) {
+                    float v[MG][8];
+                    float4 f[MG][2];
+                    size_t base[MG];
+                    bool in[MG];
+#pragma unroll
+                    for (int i = 0; i < MG; i++) {
+                        int b = 0, y = 0, x = 0;
+                        in[i] = locate(q0 + (uint32_t)((m0 + i) * 128), b, y, x);
+                        base[i] = ((size_t)b * 4 * a.gi.H + 4 * y + 2 * half) * W4 + 4 * x;
+                        if (in[i]) {
+                            f[i][0] = *reinterpret_cast<const float4 *>(a.fbp + base[i]);
+                            f[i][1] = *reinterpret_cast<const float4 *>(a.fbp + base[i] + W4);
                         }
                     }
-                    continue;
-                }
-                for (int c0 = 0; c0 < ch; c0 += 32) {
-                    float v[32];
-                    const int n = ch - c0 < 32 ? ch - c0 : 32;  // 8, 16 or 32 columns
-                    if (n == 32)
-                        tld<32>(tbase + (uint32_t)c0, v);
-                    else if (n == 16)
-                        tld<16>(tbase + (uint32_t)c0, *reinterpret_cast<float(*)[16]>(v));
-                    else
-                        tld<8>(tbase + (uint32_t)c0, *reinterpret_cast<float(*)[8]>(v));
-                    tld_wait();
-                    if (!inside) continue;
-                    const int cbase = half * ch + c0;
 #pragma unroll
-                    for (int g8 = 0; g8 < 4; g8++) {
-                        if (g8 * 8 >= n) break;
+                    for (int i = 0; i < MG; i++) tld<8>(tb + (uint32_t)((m0 + i) * Cout), v[i]);
+                    tld_wait();
+#pragma unroll
+                    for (int i = 0; i < MG; i++) {
+                        if (!in[i]) continue;
+#pragma unroll
+                        for (int dy = 0; dy < 2; dy++) {
+                            const float *bb = s_bias + 8 * half + 4 * dy;
+                            float4 o;
+                            o.x = f[i][dy].x + a.scale * (v[i][4 * dy + 0] + bb[0]);
+                            o.y = f[i][dy].y + a.scale * (v[i][4 * dy + 1] + bb[1]);
+                            o.z = f[i][dy].z + a.scale * (v[i][4 * dy + 2] + bb[2]);
+                            o.w = f[i][dy].w + a.scale * (v[i][4 * dy + 3] + bb[3]);
+                            *reinterpret_cast<float4 *>(a.img + base[i] + (size_t)dy * W4) = o;
+                        }
+                    }
+                }
+            } else if (a.mode == EPI_STORE) {
+                // interior flags of this thread's MT rows, once per tile
+                uint32_t inmask = 0;
+#pragma unroll
+                for (int m = 0; m < MT; m++) {
+                    int b, y, x;
+                    if (locate(q0 + (uint32_t)(m * 128), b, y, x)) inmask |= 1u << m;
+                }
+                // chunks of 8 channels over (row block, channel group); chunks per block is a power
+                // of two (Cout / 16); 4 chunks in flight per wait
+                const int lcpm = ilog2_dev(ch >> 3), nch = MT << lcpm;
+                for (int c0 = 0; c0 < nch; c0 += 4) {
+                    float v[4][8];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+                        if (c0 + i < nch) {
+                            const int m = (c0 + i) >> lcpm, cc = (c0 + i) & ((1 << lcpm) - 1);
+                            tld<8>(tb + (uint32_t)(m * Cout + cc * 8), v[i]);
+                        }
+                    tld_wait();
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        if (c0 + i >= nch) break;
+                        const int m = (c0 + i) >> lcpm, cc = (c0 + i) & ((1 << lcpm) - 1);
+                        if (!((inmask >> m) & 1u)) continue;
+                        const uint32_t q = q0 + (uint32_t)(m * 128);
+                        const int c = half * ch + cc * 8;
                         float w[8];
 #pragma unroll
                         for (int j = 0; j < 8; j++) {
-                            w[j] = v[g8 * 8 + j] + s_bias[cbase + g8 * 8 + j];
+                            w[j] = v[i][j] + s_bias[c + j];
                             if (a.relu) w[j] = fmaxf(w[j], 0.f);
                         }
-                        const int g = (cbase >> 3) + g8;
-                        if (a.mode == EPI_STORE) {
-                            bf16 *dst = a.out + ((size_t)g * a.gi.alloc + a.gi.guard + q) * 8;
-                            *reinterpret_cast<uint4 *>(dst) = pack8(w);
-                        } else {
-                            // nearest 2x up-sampling plus the skip tensor at the output grid; the
-                            // decoder activation is rounded to BF16 first, as where it is stored
+                        bf16 *dst = a.out + ((size_t)(c >> 3) * a.gi.alloc + a.gi.guard + q) * 8;
+                        *reinterpret_cast<uint4 *>(dst) = pack8(w);
+                    }
+                }
+            } else {
+                // decoder: nearest 2x up-sampling plus the skip tensor at the output grid; the skip loads
+                // and TMEM loads of 2 chunks are in flight before the wait.  The decoder activation is
+                // rounded to BF16 first, as where it is stored.
+                const int lcpm = ilog2_dev(ch >> 3), nch = MT << lcpm;
+                const uint32_t Wo = (uint32_t)a.go.W + 2, Ho = (uint32_t)a.go.H + 2;
+                for (int c0 = 0; c0 < nch; c0 += 2) {
+                    float v[2][8];
+                    uint4 sk[2][4];
+                    size_t off[2];
+                    bool in[2];
 #pragma unroll
-                            for (int j = 0; j < 8; j++) w[j] = __bfloat162float(__float2bfloat16(w[j]));
-                            const uint32_t Wo = (uint32_t)a.go.W + 2, Ho = (uint32_t)a.go.H + 2;
+                    for (int i = 0; i < 2; i++) {
+                        in[i] = false;
+                        if (c0 + i >= nch) continue;
+                        const int m = (c0 + i) >> lcpm, cc = (c0 + i) & ((1 << lcpm) - 1);
+                        int b = 0, y = 0, x = 0;
+                        in[i] = locate(q0 + (uint32_t)(m * 128), b, y, x);
+                        const int g = (half * ch + cc * 8) >> 3;
+                        const uint32_t qo = ((uint32_t)b * Ho + 2 * y + 1) * Wo + 2 * x + 1;
+                        off[i] = ((size_t)g * a.go.alloc + a.go.guard + qo) * 8;
+                        if (in[i]) {
+                            const bf16 *sp = a.skip + off[i];
+                            sk[i][0] = *reinterpret_cast<const uint4 *>(sp);
+                            sk[i][1] = *reinterpret_cast<const uint4 *>(sp + 8);
+                            sk[i][2] = *reinterpret_cast<const uint4 *>(sp + (size_t)Wo * 8);
+                            sk[i][3] = *reinterpret_cast<const uint4 *>(sp + (size_t)Wo * 8 + 8);
+                        }
+                    }
 #pragma unroll
-                            for (int i = 0; i < 2; i++) {
-                                const uint32_t qo = ((uint32_t)b * Ho + 2 * y + i + 1) * Wo + 2 * x + 1;
-                                const size_t off = ((size_t)g * a.go.alloc + a.go.guard + qo) * 8;
-                                const uint4 s0 = *reinterpret_cast<const uint4 *>(a.skip + off);
-                                const uint4 s1 = *reinterpret_cast<const uint4 *>(a.skip + off + 8);
-                                float o0[8], o1[8];
+                    for (int i = 0; i < 2; i++)
+                        if (c0 + i < nch) {
+                            const int m = (c0 + i) >> lcpm, cc = (c0 + i) & ((1 << lcpm) - 1);
+                            tld<8>(tb + (uint32_t)(m * Cout + cc * 8), v[i]);
+                        }
+                    tld_wait();
 #pragma unroll
-                                for (int k = 0; k < 8; k++) o0[k] = o1[k] = w[k];
-                                unpack8_add(s0, o0);
-                                unpack8_add(s1, o1);
-                                *reinterpret_cast<uint4 *>(a.out + off) = pack8(o0);
-                                *reinterpret_cast<uint4 *>(a.out + off + 8) = pack8(o1);
-                            }
+                    for (int i = 0; i < 2; i++) {
+                        if (!in[i]) continue;
+                        const int cc = (c0 + i) & ((1 << lcpm) - 1);
+                        const int c = half * ch + cc * 8;
+                        float w[8];
+#pragma unroll
+                        for (int j = 0; j < 8; j++) {
+                            w[j] = v[i][j] + s_bias[c + j];
+                            if (a.relu) w[j] = fmaxf(w[j], 0.f);
+                            w[j] = __bfloat162float(__float2bfloat16(w[j]));
+                        }
+#pragma unroll
+                        for (int r = 0; r < 4; r++) {
+                            float o[8];
+#pragma unroll
+                            for (int k = 0; k < 8; k++) o[k] = w[k];
+                            unpack8_add(sk[i][r], o);
+                            const size_t d = off[i] + (size_t)(r >> 1) * Wo * 8 + (size_t)(r & 1) * 8;
+                            *reinterpret_cast<uint4 *>(a.out + d) = pack8(o);
                         }
                     }
                 }
@@ -609,7 +690,7 @@ static ufob_status cg_alloc(CGBuf &t, int B, int H, int W, int C, cudaStream_t s
 struct FastNet {
     DevBuf wt[8];
     CGBuf x0, e1, p1, e2, p2, e3, p3, e4, u3, u2, u1;
-    int smem_attr = 0;
+    uint32_t smem_attr = 0;  // bit (3 log2 MT + log2 KS): shared-memory attribute set for that instance
 };
 
 // Tile plan of one layer: row blocks per tile (two accumulator buffers of
@@ -651,6 +732,20 @@ static ConvPlan plan_conv(int Cin, int Cout, const CGGeom &g)
     return best;
 }
 
+typedef void (*ConvKernel)(const FastConvArgs);
+
+static ConvKernel conv_kernel(int mt, int ks)
+{
+#define UFOB_CONV_CASE(M, K) \
+    if (mt == M && ks == K) return k_conv_cg<M, K>;
+    UFOB_CONV_CASE(1, 1) UFOB_CONV_CASE(1, 2) UFOB_CONV_CASE(1, 4)
+    UFOB_CONV_CASE(2, 1) UFOB_CONV_CASE(2, 2) UFOB_CONV_CASE(2, 4)
+    UFOB_CONV_CASE(4, 1) UFOB_CONV_CASE(4, 2) UFOB_CONV_CASE(4, 4)
+    UFOB_CONV_CASE(8, 1) UFOB_CONV_CASE(8, 2) UFOB_CONV_CASE(8, 4)
+#undef UFOB_CONV_CASE
+    return nullptr;
+}
+
 static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const float *bias, int Cout, int relu,
                            int mode, CGBuf *out, const CGBuf *skip, const float *fbp, float *img, float scale,
                            cudaStream_t s)
@@ -682,14 +777,28 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
     a.img = img;
     a.ntiles = pl.ntiles;
     const size_t smem = pl.smem;
-    if (!f->smem_attr) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_conv_cg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-        f->smem_attr = 1;
+    const int ks = (in.C < 64 ? in.C / 8 : 8) / 2;
+    auto kern = conv_kernel(a.MT, ks);
+    if (!kern) return fail(UFOB_ERR_UNSUPPORTED, "cnn: no convolution kernel for %d row blocks x %d K-steps", a.MT, ks);
+    const uint32_t bit = 1u << (ilog2((uint64_t)a.MT) * 3 + ilog2((uint64_t)ks));
+    if (!(f->smem_attr & bit)) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+        cudaFuncAttributes fa;
+        UFOB_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+        if (fa.maxThreadsPerBlock < kThreads)
+            return fail(UFOB_ERR_UNSUPPORTED,
+                        "cnn: convolution kernel (%d row blocks, %d K-steps) takes %d registers: at most %d threads "
+                        "per block, %d needed",
+                        a.MT, ks, fa.numRegs, fa.maxThreadsPerBlock, kThreads);
+        f->smem_attr |= bit;
     }
     // one CTA per SM: the two accumulator buffers may take all 512 TMEM columns
     const long long grid = std::min<long long>(a.ntiles, num_sms());
-    k_conv_cg<<<(unsigned)grid, kThreads, std::max<size_t>(smem, 116 * 1024), s>>>(a);
-    UFOB_CUDA_TRY(cudaGetLastError());
+    kern<<<(unsigned)grid, kThreads, std::max<size_t>(smem, 116 * 1024), s>>>(a);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess)
+        return fail(UFOB_ERR_CUDA, "cnn: convolution launch (%d row blocks, %d K-steps, %zu B shared) failed: %s", a.MT,
+                    ks, std::max<size_t>(smem, 116 * 1024), cudaGetErrorString(le));
     note_launch();
     return UFOB_OK;
 }
