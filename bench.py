@@ -382,12 +382,14 @@ def main():
 
     # roofline of the dominant kernel (backprojection)
     bp_ms, bp_n = chosen["kernel_ms_per_step"]["backproject"], chosen["kernel_launches_per_step"]["backproject"]
-    gather_bytes = 8.0 if storage == ufob.F32 else 4.0  # on-chip bytes per update: 2 FP32 taps / 1 FP16 pair
+    # on-chip bytes per update: 2 FP32 taps / one FP16 tap pair (a 16-byte cell serves 4 slices)
+    gather_bytes = 8.0 if storage == ufob.F32 else 4.0
     upd_per_launch = updates_per_step / bp_n
     avg_launch_s = bp_ms / bp_n * 1e-3
     achieved = upd_per_launch * gather_bytes / avg_launch_s / 1e9
-    traffic_per_upd = read_profile_traffic("bp_linear_c1.md")
-    roofline = {"bound": "smem", "kernel": "k_bp_linear", "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
+    bp_kernel = "k_bp_linear" if storage == ufob.F32 else "k_bp_quads"
+    traffic_per_upd = read_profile_traffic("bp_linear_c1.md" if storage == ufob.F32 else "bp_quads_c1.md")
+    roofline = {"bound": "smem", "kernel": bp_kernel, "achieved": achieved, "peak": smem_gbs, "unit": "GB/s",
                 "frac": achieved / smem_gbs,
                 "traffic": traffic_per_upd * upd_per_launch if traffic_per_upd is not None else None,
                 "algorithmic_bytes_per_update": gather_bytes,
@@ -402,7 +404,7 @@ def main():
     except Exception:
         pass
     f_ms, f_n = chosen["kernel_ms_per_step"]["filter"], chosen["kernel_launches_per_step"]["filter"]
-    f_bytes = Z * P * W * 4.0 + Z * P * (W if storage == ufob.F32 else (W + 4)) * 4.0
+    f_bytes = Z * P * W * 4.0 + Z * P * (W if storage == ufob.F32 else (W + 1)) * 4.0
     roofline_filter = {"bound": "hbm", "kernel": "k_filter_rows", "achieved": f_bytes / (f_ms * 1e-3) / 1e9,
                        "peak": hbm_peak, "unit": "GB/s",
                        "frac": (f_bytes / (f_ms * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,

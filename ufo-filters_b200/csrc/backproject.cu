@@ -758,15 +758,22 @@ __device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPAr
 }
 
 template <int TX, int TY, int ZT, int A, int S, int ACC, bool KAHAN>
-__global__ void __launch_bounds__(256) k_bp_quads(const __grid_constant__ CUtensorMap map, const BPArgs args)
+__global__ void __launch_bounds__(256, 2) k_bp_quads(const __grid_constant__ CUtensorMap map, const BPArgs args)
 {
     using Sh = BPQShape<TX, TY, ZT, A, S>;
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     const BPSmem<Sh> sm(smem_dyn);
     init_ring<S>(sm.full);
     uint32_t g = 0;
-    bp_tile_quads<TX, TY, ZT, A, S, ACC, KAHAN>(&map, args, blockIdx.x * TX, blockIdx.y * TY, blockIdx.z * ZT, sm,
-                                                 g);
+    // Tiles in bands of 16 tile columns, walked top to bottom: the CTAs resident at one time cover
+    // a compact region whose projection spans ~30% of the detector instead of a full-width strip
+    // (which re-read a whole 16-slice group, larger than L2, once per wave).
+    constexpr int GW = 16;
+    const int id = blockIdx.y * gridDim.x + blockIdx.x, band_tiles = GW * gridDim.y;
+    const int band = id / band_tiles, r = id - band * band_tiles;
+    const int bw = min(GW, (int)gridDim.x - band * GW);
+    const int tx = band * GW + r % bw, ty = r / bw;
+    bp_tile_quads<TX, TY, ZT, A, S, ACC, KAHAN>(&map, args, tx * TX, ty * TY, blockIdx.z * ZT, sm, g);
 }
 
 // ------------------------------------------------------------------ nearest kernel

@@ -79,6 +79,17 @@ class SparseViewNet:
         self.scale = scale
         self.n_params = int(lib().ufob_cnn_num_params())
 
+    @classmethod
+    def pretrained(cls, path=None):
+        """The network trained by `python -m ufob.train_cnn` (20k engine-made pairs,
+        512^2, 90 -> 1800 angles), shipped as weights/sparse_view_90to1800_512.npz."""
+        path = path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
+                                    "sparse_view_90to1800_512.npz")
+        d = np.load(path)
+        net = cls(seed=0, scale=float(d["scale"]))
+        net.set_state(PARAMS, d["params"])
+        return net
+
     def forward(self, fbp, out=None, stream=None):
         """[B, H, W] FP32 CUDA tensor (sides multiples of 32) -> corrected slices."""
         import torch

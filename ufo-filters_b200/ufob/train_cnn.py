@@ -127,7 +127,7 @@ def main(argv=None):
     report["eval"] = {"seeds": [args.eval_base, args.eval_base + args.eval_count],
                       "plain_fbp90_rel_l2": round(float(torch.cat(e_plain).mean()), 5),
                       "cnn_rel_l2": round(float(torch.cat(e_net).mean()), 5)}
-    report["time_per_slice"] = time_paths(net, maker)
+    report["time_per_slice"] = [time_paths(net, maker, B=b) for b in (64, 128)]
     print(json.dumps(report))
 
 
