@@ -20,9 +20,12 @@
 // The tables are built on the device in FP64 (one thread per projection, or
 // per projection and slice when the swept parameter is not z) and cast to the
 // compute type.  The backprojection kernel gives each thread a column of ZT
-// voxels along z, so the x/y part of every dot product is formed once per
-// projection; table blocks are staged in shared memory; interpolation uses
-// exact FP32 weights with the reference's addressing modes.
+// voxels along z (8 cone, 4 otherwise), so the x/y part of every dot product is
+// formed once per projection; table blocks are staged in shared memory.  With
+// the FP32 compute type each sample is one texture gather of the 2x2 footprint
+// (texture border/clamp addressing = the reference's CLAMP / CLAMP_TO_EDGE) and
+// the cone divisions are approximate reciprocals; interpolation weights are
+// exact FP32 in every path.
 #include <cuda_fp16.h>
 #include <math.h>
 
@@ -246,6 +249,62 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, int W, 
     return fmaf(b, bot - top, top);
 }
 
+// Fast path of bilinear() for FP32 coordinates: floor and fraction from the
+// 1.5 * 2^23 rounding trick (i = rint(x - 1) with x = coordinate, which is
+// floor(x - 0.5) except at exact ties, where the fraction becomes 1 and the
+// interpolated value is the same), no float-to-int conversion.  Coordinates
+// beyond +-4e6 (outside any detector) and NaN take the general path.
+__device__ __forceinline__ float bilinear_fast(const float *__restrict__ img, int W, int H, float u, float v,
+                                               int addr)
+{
+    const float M = 12582912.0f;  // 1.5 * 2^23
+    if (!(fabsf(u) < 4.0e6f && fabsf(v) < 4.0e6f)) return bilinear<float>(img, W, H, u, v, addr);
+    const float ru = u + (M - 1.0f), rv = v + (M - 1.0f);
+    const int i = __float_as_int(ru) - __float_as_int(M), j = __float_as_int(rv) - __float_as_int(M);
+    const float a = (u - 0.5f) - (ru - M), b = (v - 0.5f) - (rv - M);
+    float t00, t10, t01, t11;
+    if ((unsigned)i < (unsigned)(W - 1) && (unsigned)j < (unsigned)(H - 1)) {
+        const float *q = img + (size_t)j * W + i;
+        t00 = __ldg(q);
+        t10 = __ldg(q + 1);
+        t01 = __ldg(q + W);
+        t11 = __ldg(q + W + 1);
+    } else {
+        t00 = texel(img, W, H, i, j, addr);
+        t10 = texel(img, W, H, i + 1, j, addr);
+        t01 = texel(img, W, H, i, j + 1, addr);
+        t11 = texel(img, W, H, i + 1, j + 1, addr);
+    }
+    const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
+    return fmaf(b, bot - top, top);
+}
+
+// Bilinear sample through the texture unit: tex2Dgather returns the 2x2
+// footprint (x: (i0, j0+1), y: (i0+1, j0+1), z: (i0+1, j0), w: (i0, j0)).  It is
+// queried at the centre of the footprint chosen here in software, so the
+// texel selection never depends on the unit's coordinate rounding; the weights
+// are exact FP32.  The texture's border (0) / clamp addressing implements the
+// reference's CLAMP / CLAMP_TO_EDGE; coordinates are first clamped to
+// [-2, size + 2], which leaves both modes' results unchanged.
+__device__ __forceinline__ float bilinear_tex(cudaTextureObject_t t, int W, int H, float u, float v)
+{
+    const float M = 12582912.0f;  // 1.5 * 2^23
+    u = fminf(fmaxf(u, -2.0f), (float)W + 2.0f);
+    v = fminf(fmaxf(v, -2.0f), (float)H + 2.0f);
+    const float fu = (u + (M - 1.0f)) - M, fv = (v + (M - 1.0f)) - M;  // rint(u - 1) = floor(u - 0.5) but ties
+    const float a = (u - 0.5f) - fu, b = (v - 0.5f) - fv;
+    const float4 g = tex2Dgather<float4>(t, fu + 1.0f, fv + 1.0f, 0);
+    const float top = fmaf(a, g.z - g.w, g.w), bot = fmaf(a, g.y - g.x, g.x);
+    return fmaf(b, bot - top, top);
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // ---------------------------------------------------------------- accumulation semantics
 
 struct StoreParams {
@@ -307,13 +366,14 @@ struct GBPArgs {
     StoreParams sp;
     int addr;
     void *vol;
+    const cudaTextureObject_t *tex;  // one per projection (FP32 compute type), or null: global loads
 };
 
-template <bool CONE, typename CT, int RT, bool PARAMZ, int ZT>
+template <bool CONE, typename CT, int RT, bool PARAMZ, int ZT, bool TEX>
 __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
 {
     constexpr int PB = 16;  // projections per staged table block
-    __shared__ CT s_tab[PB * kTab];
+    __shared__ __align__(16) CT s_tab[PB * kTab];
     const int ix = blockIdx.x * 32 + (threadIdx.x & 31);
     const int iy = blockIdx.y * 8 + (threadIdx.x >> 5);
     const int z0 = blockIdx.z * ZT;
@@ -337,8 +397,19 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
         for (uint32_t i = threadIdx.x; i < nb * kTab; i += blockDim.x) s_tab[i] = tab[(size_t)p0 * kTab + i];
         __syncthreads();
         for (uint32_t q = 0; q < nb; q++) {
-            const CT *t = s_tab + q * kTab;
+            CT t[kTab];
+            if (sizeof(CT) == 4) {
+                // the projection's table as five 16-byte shared loads (broadcast)
+#pragma unroll
+                for (int r = 0; r < kTab / 4; r++)
+                    *reinterpret_cast<float4 *>(&t[4 * r]) = reinterpret_cast<const float4 *>(s_tab + q * kTab)[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < kTab; r++) t[r] = s_tab[q * kTab + r];
+            }
             const float *img = a.proj + (size_t)(p0 + q) * plane;
+            cudaTextureObject_t tx = 0;
+            if (TEX) tx = a.tex[p0 + q];
             const CT u_xy = fmaf_ct(t[0], fx, fmaf_ct(t[1], fy, t[3]));
             const CT v_xy = fmaf_ct(t[4], fx, fmaf_ct(t[5], fy, t[7]));
             CT d_xy = (CT)1, c_xy = (CT)1;
@@ -351,13 +422,24 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
                 CT u = fmaf_ct(t[2], zv[k], u_xy), v = fmaf_ct(t[6], zv[k], v_xy);
                 CT wgt = (CT)1;
                 if (CONE) {
-                    const CT inv = (CT)1 / fmaf_ct(t[10], zv[k], d_xy);
-                    u *= inv;
-                    v *= inv;
-                    const CT cc = t[16] / fmaf_ct(t[14], zv[k], c_xy);
-                    wgt = cc * cc;
+                    if (sizeof(CT) == 4) {
+                        // approximate reciprocals (1 ulp): u = Nu.X / D.X, weight = (K / C.X)^2
+                        const float inv = rcp_approx((float)fmaf_ct(t[10], zv[k], d_xy));
+                        u *= (CT)inv;
+                        v *= (CT)inv;
+                        const float cc = (float)t[16] * rcp_approx((float)fmaf_ct(t[14], zv[k], c_xy));
+                        wgt = (CT)(cc * cc);
+                    } else {
+                        const CT inv = (CT)1 / fmaf_ct(t[10], zv[k], d_xy);
+                        u *= inv;
+                        v *= inv;
+                        const CT cc = t[16] / fmaf_ct(t[14], zv[k], c_xy);
+                        wgt = cc * cc;
+                    }
                 }
-                const float val = bilinear<CT>(img, (int)a.W, (int)a.H, u, v, a.addr);
+                const float val = TEX ? bilinear_tex(tx, (int)a.W, (int)a.H, (float)u, (float)v)
+                                  : sizeof(CT) == 4 ? bilinear_fast(img, (int)a.W, (int)a.H, (float)u, (float)v, a.addr)
+                                                    : bilinear<CT>(img, (int)a.W, (int)a.H, u, v, a.addr);
                 result_add<RT, CT>(bsum[k], CONE ? (CT)val * wgt : (CT)val);
             }
             if (++in_burst == a.burst || p0 + q + 1 == a.n_proj) {
@@ -381,9 +463,14 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
 template <bool CONE, typename CT, int RT, bool PARAMZ>
 static ufob_status launch_gbp_t(const GBPArgs &a, cudaStream_t s)
 {
-    constexpr int ZT = PARAMZ ? 4 : 1;
+    // voxels per thread along z: 8 for cone beam (two reciprocals per sample make the per-voxel
+    // x/y work worth sharing), 4 otherwise (fewer detector rows per warp); measured on B200
+    constexpr int ZT = PARAMZ ? (CONE ? 8 : 4) : 1;
     dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + ZT - 1) / ZT);
-    k_gbp<CONE, CT, RT, PARAMZ, ZT><<<grid, 256, 0, s>>>(a);
+    if (a.tex)
+        k_gbp<CONE, CT, RT, PARAMZ, ZT, true><<<grid, 256, 0, s>>>(a);
+    else
+        k_gbp<CONE, CT, RT, PARAMZ, ZT, false><<<grid, 256, 0, s>>>(a);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
@@ -468,12 +555,80 @@ struct ufob_gbp {
     DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol;
     uint32_t pushed = 0, pw = 0, ph = 0;
     bool volume_ready = false;
+    // texture objects over the projections of the last call (rebuilt when base/shape/mode change)
+    std::vector<cudaTextureObject_t> tex;
+    DevBuf d_tex;
+    const float *tex_base = nullptr;
+    uint32_t tex_w = 0, tex_h = 0;
+    int tex_addr = -1;
     ufob_gbp()
     {
         for (int i = 0; i < GC_NCOLS; i++) geom[i] = {0.0};
         geom[GC_SRC_Y] = {-INFINITY};
     }
+    void drop_textures()
+    {
+        for (cudaTextureObject_t t : tex) cudaDestroyTextureObject(t);
+        tex.clear();
+        tex_base = nullptr;
+    }
+    ~ufob_gbp() { drop_textures(); }
 };
+
+// One 2-D texture object per projection of a [n][H][W] FP32 stack (pitch W * 4
+// bytes), border or clamp addressing, point sampling (the gather path).
+// Returns false when the stack does not meet the texture alignment rules.
+static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H, uint32_t n, int addr,
+                         cudaStream_t s)
+{
+    if (g->tex_base == base && g->tex_w == W && g->tex_h == H && g->tex.size() == n && g->tex_addr == addr)
+        return true;
+    g->drop_textures();
+    int dev = 0, align = 0, palign = 0, maxw = 0, maxh = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&palign, cudaDevAttrTexturePitchAlignment, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture2DLinearWidth, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&maxh, cudaDevAttrMaxTexture2DLinearHeight, dev) != cudaSuccess)
+        return false;
+    const size_t plane = (size_t)W * H * sizeof(float);
+    if (((uintptr_t)base % align) || (plane % align) || ((W * sizeof(float)) % palign) || W > (uint32_t)maxw ||
+        H > (uint32_t)maxh || W < 2 || H < 2)
+        return false;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = addr == AD_CLAMP ? cudaAddressModeBorder : cudaAddressModeClamp;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    g->tex.reserve(n);
+    for (uint32_t p = 0; p < n; p++) {
+        cudaResourceDesc rd = {};
+        rd.resType = cudaResourceTypePitch2D;
+        rd.res.pitch2D.devPtr = const_cast<float *>(base) + (size_t)p * W * H;
+        rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+        rd.res.pitch2D.width = W;
+        rd.res.pitch2D.height = H;
+        rd.res.pitch2D.pitchInBytes = W * sizeof(float);
+        cudaTextureObject_t t = 0;
+        if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
+            cudaGetLastError();
+            g->drop_textures();
+            return false;
+        }
+        g->tex.push_back(t);
+    }
+    if (g->d_tex.ensure(n * sizeof(cudaTextureObject_t)) != UFOB_OK ||
+        cudaMemcpyAsync(g->d_tex.ptr, g->tex.data(), n * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess) {
+        g->drop_textures();
+        return false;
+    }
+    g->tex_base = base;
+    g->tex_w = W;
+    g->tex_h = H;
+    g->tex_addr = addr;
+    return true;
+}
 
 static int geom_col(const char *name)
 {
@@ -694,6 +849,7 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
     a.sp.gray_scale = g->store_type >= ST_UCHAR ? maxv / (g->gray_map_max - g->gray_map_min) : 0.0;
     a.addr = g->addressing_mode == AD_CLAMP ? AD_CLAMP : AD_CLAMP_TO_EDGE;  // "none": defined as clamp-to-edge
     a.vol = d_vol;
+    a.tex = nullptr;
     const bool cone = !parallel;
     if (g->compute_type == 1) {
         a.tab = g->d_tab_d.ptr;
@@ -701,6 +857,7 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
                     : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
     }
     a.tab = g->d_tab_f.ptr;
+    if (gbp_textures(g, d_proj, W, H, n, a.addr, s)) a.tex = g->d_tex.as<cudaTextureObject_t>();
     return cone ? launch_gbp_rt<true, float>(a, g->result_type, paramz, s)
                 : launch_gbp_rt<false, float>(a, g->result_type, paramz, s);
 }

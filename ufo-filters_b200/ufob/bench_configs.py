@@ -89,11 +89,15 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gbp", action="store_true", help="only the general backprojection")
     ap.add_argument("--batch", action="store_true", help="only the uneven batch")
+    ap.add_argument("--projections", type=int, default=1024)
+    ap.add_argument("--detector", type=int, default=1024)
+    ap.add_argument("--volume", type=int, default=512)
+    ap.add_argument("--reps", type=int, default=2)
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
     if not args.batch:
-        rows += bench_gbp()
+        rows += bench_gbp(args.reps, args.projections, args.detector, args.volume)
     if not args.gbp:
         rows += bench_batch()
     device_status()
