@@ -200,3 +200,33 @@ def evaluate(net, seeds, maker=None, batch=16):
         e_net.append(rel_l2(out, y))
     torch.cuda.synchronize()
     return float(torch.cat(e_plain).mean()), float(torch.cat(e_net).mean())
+
+
+def _main(argv=None):
+    """python -m ufob.cnn [--batch B] [--reps R]: time the inference path on
+    B random 512^2 slices (the shipped weights), one JSON line."""
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--reps", type=int, default=5)
+    args = ap.parse_args(argv)
+    net = SparseViewNet.pretrained()
+    x = torch.randn(args.batch, 512, 512, device="cuda") * 0.3
+    net.forward(x)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.reps):
+        net.forward(x)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.reps
+    flop = 1.208e9 * args.batch  # sum over the 8 convolutions of 2 * 9 * Cin * Cout * H * W
+    print(json.dumps({"workload": "sparse-view network forward, %d x 512^2" % args.batch, "ms": round(ms, 3),
+                      "us_per_slice": round(ms * 1e3 / args.batch, 2), "tflops": round(flop / ms / 1e9, 1)}))
+
+
+if __name__ == "__main__":
+    _main()
