@@ -250,27 +250,11 @@ def main():
     import torch
     import ufob
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    from ufob import dist as udist
+    # one process per GPU (torchrun env), independent slices per rank, NCCL only for the timing reductions
+    ctx = udist.init(timeout_s=600)
+    world, rank, dev = ctx.world, ctx.rank, ctx.device
+    barrier, max_over_ranks = ctx.barrier, ctx.max_over_ranks
 
     Z, P, W = args.slices, args.angles, args.width
     updates_per_step = float(Z) * W * W * P
@@ -431,8 +415,7 @@ def main():
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    udist.finish(ctx)
 
 
 if __name__ == "__main__":
