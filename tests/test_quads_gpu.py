@@ -59,7 +59,7 @@ def test_quads_backprojection(cuda, half_sums, tol, kahan, nz):
         assert oracle.rel_l2(got[z], ref[z]) < tol, z
 
 
-@pytest.mark.parametrize("tile", list(range(8)) + [16, 19])
+@pytest.mark.parametrize("tile", list(range(13)) + [16, 19])
 def test_quads_tiles(cuda, tile):
     W, P, nz = 200, 180, 8
     raw = _raw(nz, P, W, 5)

@@ -985,11 +985,13 @@ static ufob_status quads_tile(int tile, const BPGeometry &g, const void *d, uint
     case 8: return launch_quads_t<32, 16, 16, 16, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
     case 9: return launch_quads_t<32, 16, 16, 8, 3, ACC, KAHAN>(g, d, pitch, gp, o, s);
     case 10: return launch_quads_t<32, 8, 16, 16, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 11: return launch_quads_t<32, 8, 32, 8, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
+    case 12: return launch_quads_t<32, 8, 32, 16, 2, ACC, KAHAN>(g, d, pitch, gp, o, s);
     default: return fail(UFOB_ERR_INVALID, "backproject: unknown slice-quad tile id %d", tile);
     }
 }
 
-int bp_quad_tiles() { return 11; }
+int bp_quad_tiles() { return 13; }
 
 // Slice-quad FP16 backprojection.  pitch = cells per angle row (>= W + 1),
 // group_pitch = cells per group of four slices (>= P * pitch).  `tile` < 0
