@@ -281,6 +281,88 @@ ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint32_t n, void
 int ufob_batch_variant(ufob_batch *b);
 void ufob_batch_destroy(ufob_batch *b);
 
+/* ---------------------------------------------------------- preprocessing
+ * The tasks in front of `fft` in a reconstruction graph, each on its own and
+ * fused into the filter stage's row loads (ufob_filter_run_projections,
+ * ufob_fbp_run_projections), so raw projections go to filtered sinograms in
+ * one pass over HBM.
+ *
+ * flat-field-correct: replaces src/ufo-flat-field-correct-task.c:120-170 and
+ * src/kernels/ffc.cl:20-50.  Properties (names, defaults as the reference): */
+typedef struct {
+    int fix_nan_and_inf;    /* "fix-nan-and-inf", default 0: NaN/Inf results become 0 */
+    int absorption_correct; /* "absorption-correct", default 0: log(flat' / data') instead of data' / flat' */
+    int sinogram_input;     /* "sinogram-input", default 0: dark and flat are one row of `width` */
+    float dark_scale;       /* "dark-scale", default 1.0 */
+    float flat_scale;       /* "flat-scale", default 1.0 */
+} ufob_ffc_props;
+void ufob_ffc_props_init(ufob_ffc_props *props);
+/* Set one property by its reference name (booleans as 0/1). */
+ufob_status ufob_ffc_set_property(ufob_ffc_props *props, const char *name, double value);
+/* n_frames frames [n_frames][height][width] (or sinograms with sinogram_input)
+ * corrected with one dark and one flat frame [height][width] (one row [width]
+ * with sinogram_input): out = (data - dark * dark_scale) / (flat * flat_scale -
+ * dark * dark_scale), or the log of the inverse ratio with absorption_correct. */
+ufob_status ufob_flat_field_correct(const ufob_ffc_props *props, const float *d_data, const float *d_dark,
+                                    const float *d_flat, uint32_t width, uint32_t height, uint32_t n_frames,
+                                    float *d_out, void *stream);
+
+/* cone-beam-projection-weight: replaces
+ * src/ufo-cone-beam-projection-weight-task.c:113-151 and
+ * src/kernels/conebeam.cl:20-36.  Array properties "center-position-x",
+ * "center-position-z", "source-distance", "detector-distance" (no default: they
+ * must be set) and "axis-angle-x" (default 0); a single value broadcasts, else
+ * projection i uses value i.  The handle counts the projections it has weighted,
+ * as the task's process() counter does. */
+typedef struct ufob_cone_weight ufob_cone_weight;
+ufob_status ufob_cone_weight_create(ufob_cone_weight **out);
+ufob_status ufob_cone_weight_set_array(ufob_cone_weight *w, const char *name, const double *values, uint32_t n);
+ufob_status ufob_cone_weight_set_property(ufob_cone_weight *w, const char *name, double value);
+/* Weight projections [n][height][width] (projection indices count .. count+n-1;
+ * count advances by n).  d_out may equal d_in. */
+ufob_status ufob_cone_weight_run(ufob_cone_weight *w, const float *d_in, uint32_t width, uint32_t height,
+                                 uint32_t n, float *d_out, void *stream);
+/* Projection index the next run starts at (0 after create). */
+ufob_status ufob_cone_weight_set_count(ufob_cone_weight *w, uint32_t count);
+uint32_t ufob_cone_weight_get_count(const ufob_cone_weight *w);
+void ufob_cone_weight_destroy(ufob_cone_weight *w);
+
+/* transpose-projections: replaces src/ufo-transpose-projections-task.c:60-120
+ * (an OpenMP row copy on the host there).  Projections [n][height][width] become
+ * projections first .. first+n-1 of `height` sinograms [height][n_total][width]. */
+ufob_status ufob_transpose_projections(const float *d_proj, uint32_t width, uint32_t height, uint32_t n,
+                                       float *d_sinos, uint32_t n_total, uint32_t first, void *stream);
+
+/* Preprocessing fused into a filter run.  NULL members switch a step off. */
+typedef struct {
+    const ufob_ffc_props *ffc;  /* flat-field correction with d_dark, d_flat */
+    const float *d_dark;        /* [height][width], or [width] with ffc->sinogram_input */
+    const float *d_flat;
+    ufob_cone_weight *cone;     /* cone-beam weight; its count advances by n_projections */
+} ufob_preprocess;
+
+/* Filter projections [n_projections][height][width] (row pitch `pitch`, 0 =
+ * width) after the steps of `pre` (NULL = none), for detector rows first_row ..
+ * first_row + n_rows - 1 (n_rows 0 = the rest).
+ *   sinograms = 0: output rows in projection order [n_projections][n_rows][..]
+ *     (the FDK order: cone-beam-projection-weight ! fft ! filter ! ifft);
+ *   sinograms = 1: output sinograms [n_rows][n_projections][..], i.e. the
+ *     transpose-projections step fused into the loads; out_layout QUADS gives
+ *     the slice-quad cells of that sinogram stack.
+ * Output layouts and pitches as ufob_filter_run / ufob_filter_run_quads. */
+ufob_status ufob_filter_run_projections(ufob_filter *f, const ufob_preprocess *pre, const float *d_proj,
+                                        uint32_t width, uint32_t height, uint32_t n_projections, uint32_t pitch,
+                                        int sinograms, uint32_t first_row, uint32_t n_rows, void *d_out,
+                                        ufob_dtype out_dtype, ufob_layout out_layout, uint32_t out_pitch,
+                                        void *stream);
+/* `flat-field-correct ! transpose-projections ! fft ! filter ! ifft !
+ * backproject` for detector rows first_row .. first_row + n_rows - 1 (n_rows 0 =
+ * all) of projections [n_projections][height][width] on the device: one
+ * reconstructed slice per detector row, [n_rows][roi_h][roi_w]. */
+ufob_status ufob_fbp_run_projections(ufob_fbp *fbp, const ufob_preprocess *pre, const float *d_proj,
+                                     uint32_t width, uint32_t height, uint32_t n_projections, uint32_t first_row,
+                                     uint32_t n_rows, float *d_out, void *stream);
+
 /* ------------------------------------------------------------- utilities */
 /* Analytic parallel-beam projection of ellipses (rows cx, cy, a, b, phi, rho
  * in units where the reconstruction circle has radius 1) into [P][W] float

@@ -15,6 +15,12 @@ It restates in NumPy/FP64 what the reference ufo-filters tasks compute:
 * ``backproject`` -- src/ufo-backproject-task.c:96-150,174-267 and
   src/kernels/backproject.cl:24-94 (via the C oracle).
 * ``general_backproject`` -- src/ufo-general-backproject-task.c (via the C oracle).
+* ``flat_field_correct`` -- src/kernels/ffc.cl:20-50 with the task's arguments
+  (src/ufo-flat-field-correct-task.c:120-170), in FP32.
+* ``transpose_projections`` -- src/ufo-transpose-projections-task.c:60-120.
+* ``cone_weight_params`` / ``cone_beam_weight`` --
+  src/ufo-cone-beam-projection-weight-task.c:113-151 and
+  src/kernels/conebeam.cl:20-36, in FP32.
 
 The heavy loops live in ``ufob_oracle.c`` (built into ``liboracle.so`` by the
 Makefile next to this file).
@@ -384,6 +390,88 @@ def forwardproject(slice_img, n_angles, axis_pos, angle_step):
     out = np.zeros((n_angles, W), dtype=np.float64)
     lib().oracle_forwardproject(_p(img), W, n_angles, float(axis_pos), float(angle_step), _p(out))
     return out
+
+
+# --------------------------------------------------------------------------- preprocessing
+
+def flat_field_correct(data, dark, flat, absorption_correct=False, fix_nan_and_inf=False, sinogram_input=False,
+                       dark_scale=1.0, flat_scale=1.0):
+    """src/kernels/ffc.cl:31-47 in FP32, one rounding per operation: dark/flat
+    [H, W] broadcast over frames [..., H, W] (one row [W] with sinogram-input,
+    where the kernel indexes them by the column alone, :33)."""
+    f32 = np.float32
+    d = np.asarray(data, dtype=f32)
+    dark, flat = np.asarray(dark, dtype=f32), np.asarray(flat, dtype=f32)
+    if sinogram_input:
+        dark, flat = dark.reshape(-1), flat.reshape(-1)
+    cd = dark * f32(dark_scale)
+    cf = flat * f32(flat_scale)
+    with np.errstate(all="ignore"):
+        if absorption_correct:
+            r = np.log((cf - cd) / (d - cd))
+        else:
+            r = (d - cd) / (cf - cd)
+    r = r.astype(f32)
+    if fix_nan_and_inf:  # :42-44
+        r = np.where(np.isfinite(r), r, f32(0.0))
+    return r
+
+
+def transpose_projections(proj):
+    """Projections [N, H, W] -> sinograms [H, N, W] (row y of projection p is row
+    p of sinogram y, src/ufo-transpose-projections-task.c:76-97)."""
+    return np.ascontiguousarray(np.transpose(np.asarray(proj, dtype=np.float32), (1, 0, 2)))
+
+
+def _scarray_value(values, index):
+    """ufo_scarray_get_double (src/common/ufo-scarray.c:118-127): one value
+    broadcasts, else the value at `index` (which must exist)."""
+    v = np.atleast_1d(np.asarray(values, dtype=np.float64))
+    if v.size == 1:
+        return float(v[0])
+    if index >= v.size:
+        raise IndexError("scalar array has %d values, index %d" % (v.size, index))
+    return float(v[index])
+
+
+def cone_weight_params(index, center_position_x, center_position_z, source_distance, detector_distance,
+                       axis_angle_x=0.0):
+    """FP32 kernel arguments of projection `index`
+    (src/ufo-cone-beam-projection-weight-task.c:128-139): center, source
+    distance, overall distance, magnification reciprocal, cos of the axis angle."""
+    f32 = np.float32
+    cs = f32(math.cos(_scarray_value(axis_angle_x, index)))
+    cx = f32(_scarray_value(center_position_x, index))
+    cz = f32(_scarray_value(center_position_z, index))
+    sd = f32(_scarray_value(source_distance, index))
+    dd = f32(_scarray_value(detector_distance, index))
+    od = f32(sd + dd)
+    mr = f32(sd / od)
+    if cs > f32(0.9999999):
+        od = sd
+    return cx, cz, sd, od, mr, cs
+
+
+def cone_beam_weight(proj, first=0, **props):
+    """src/kernels/conebeam.cl:20-36 for projections [n, H, W] (indices first ..
+    first+n-1) in FP32; props are the task's array properties."""
+    f32 = np.float32
+    p3 = np.asarray(proj, dtype=f32)
+    squeeze = p3.ndim == 2
+    if squeeze:
+        p3 = p3[None]
+    n, H, W = p3.shape
+    out = np.empty_like(p3)
+    kw = {k.replace("-", "_"): v for k, v in props.items()}
+    idx = np.arange(W, dtype=f32)
+    idy = np.arange(H, dtype=f32)[:, None]
+    for i in range(n):
+        cx, cz, sd, od, mr, cs = cone_weight_params(first + i, **kw)
+        x = ((idx - cx) + f32(0.5)) * mr
+        y = ((idy - cz) + f32(0.5)) * mr
+        den = np.sqrt((od * od + x * x) + y * y)
+        out[i] = ((p3[i] * sd) * cs) / den
+    return out[0] if squeeze else out
 
 
 # --------------------------------------------------------------------------- phantoms

@@ -306,6 +306,38 @@ ufob_status ufob_filter_run_quads(ufob_filter *f, const float *d_in, uint32_t wi
     return filter_quads_launch(f->plan, d_in, width, height, nslices, in_pitch, d_out, w, out_pitch, s);
 }
 
+ufob_status ufob_filter_run_projections(ufob_filter *f, const ufob_preprocess *pre, const float *d_proj,
+                                        uint32_t width, uint32_t height, uint32_t n_projections, uint32_t pitch,
+                                        int sinograms, uint32_t first_row, uint32_t n_rows, void *d_out,
+                                        ufob_dtype out_dtype, ufob_layout out_layout, uint32_t out_pitch,
+                                        void *stream)
+{
+    if (!f || !d_proj || !d_out) return fail(UFOB_ERR_INVALID, "filter_run_projections: NULL argument");
+    UFOB_TRY(ensure_device());
+    uint32_t n, w;
+    UFOB_TRY(filter_sizes(f->props, width, &n, &w));
+    cudaStream_t s = (cudaStream_t)stream;
+    UFOB_TRY(filter_plan_build(f->props, n, f->plan, s));
+    if (!pitch) pitch = width;
+    if (pitch < width) return fail(UFOB_ERR_INVALID, "filter: input pitch %u < width %u", pitch, width);
+    if (first_row > height) return fail(UFOB_ERR_INVALID, "filter: first row %u beyond height %u", first_row, height);
+    if (!n_rows) n_rows = height - first_row;
+    if (out_layout == UFOB_LAYOUT_QUADS && !sinograms)
+        return fail(UFOB_ERR_INVALID, "filter: the QUADS layout holds sinograms (sinograms = 1)");
+    if (!n_projections || !n_rows) return UFOB_OK;
+    RowSource src;
+    UFOB_TRY(projection_source(pre, d_proj, width, height, n_projections, pitch, sinograms != 0, first_row, n_rows,
+                               src, s));
+    if (out_layout == UFOB_LAYOUT_QUADS) {
+        if (out_dtype != UFOB_F16) return fail(UFOB_ERR_INVALID, "filter: the QUADS layout is F16 only");
+        if (!out_pitch) out_pitch = w + 1;
+        return filter_quads_launch_src(f->plan, src, width, n_projections, n_rows, d_out, w, out_pitch, s);
+    }
+    if (!out_pitch) out_pitch = out_layout == UFOB_LAYOUT_PAIRS ? round_up(w + 1, 4) : w;
+    return filter_rows_launch_src(f->plan, src, width, n_projections * n_rows, d_out, out_dtype, out_layout, w,
+                                  out_pitch, s);
+}
+
 ufob_status ufob_filter_coefficients(ufob_filter *f, uint32_t width, float *host_out, uint32_t count)
 {
     if (!f || !host_out) return fail(UFOB_ERR_INVALID, "filter_coefficients: NULL argument");
@@ -508,7 +540,7 @@ extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_
             return fail(UFOB_ERR_INVALID, "backproject: mode=nearest needs an F32 sinogram");
         if (!pitch) pitch = width + 1;
         if (!slice_pitch) slice_pitch = (uint64_t)pitch * height;
-        // tile ids 16..23: the same shapes with the FP16-lerp accumulation (measurement aid)
+        // tile ids 16 and up: the same shapes with the FP16-lerp accumulation (measurement aid)
         int tile = bp->props.tile, acc = bp->props.half_sums ? 2 : 0;
         if (tile >= 16) {
             acc = 1;
@@ -617,8 +649,9 @@ extern "C" ufob_status ufob_fbp_get_requisition(ufob_fbp *x, uint32_t width, uin
     return ufob_backproject_get_requisition(x->bp, fw, fh, ow, oh);
 }
 
-// Filter + backproject `nz` slices already on the device.
-static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, uint32_t height, uint32_t nz,
+// Filter + backproject `nz` slices already on the device; logical row
+// slice * height + angle of `src` is sinogram row `angle` of slice `slice`.
+static ufob_status fbp_group(ufob_fbp *x, const RowSource &src, uint32_t width, uint32_t height, uint32_t nz,
                              float *d_out, cudaStream_t s)
 {
     uint32_t nfft, fw;
@@ -640,10 +673,10 @@ static ufob_status fbp_group(ufob_fbp *x, const float *d_sino, uint32_t width, u
     }
     const ufob_layout layout = quads ? UFOB_LAYOUT_QUADS : pairs ? UFOB_LAYOUT_PAIRS : UFOB_LAYOUT_ROWS;
     if (quads)
-        UFOB_TRY(filter_quads_launch(x->f->plan, d_sino, width, height, nz, width, x->work.ptr, fw, pitch, s));
+        UFOB_TRY(filter_quads_launch_src(x->f->plan, src, width, height, nz, x->work.ptr, fw, pitch, s));
     else
-        UFOB_TRY(filter_rows_launch(x->f->plan, d_sino, width, height * nz, width, x->work.ptr, x->storage, layout, fw,
-                                    pitch, s));
+        UFOB_TRY(filter_rows_launch_src(x->f->plan, src, width, height * nz, x->work.ptr, x->storage, layout, fw,
+                                        pitch, s));
     if (x->timing) UFOB_CUDA_TRY(cudaEventRecord(e1, s));
     UFOB_TRY(ufob_backproject_run(x->bp, x->work.ptr, x->storage, layout, fw, height, nz, pitch,
                                   (uint64_t)pitch * height, d_out, s));
@@ -709,8 +742,34 @@ extern "C" ufob_status ufob_fbp_run(ufob_fbp *x, const float *d_sino, uint32_t w
     const uint32_t G = group_slices(width, height, nslices);
     for (uint32_t z = 0; z < nslices; z += G) {
         const uint32_t nz = std::min(G, nslices - z);
-        UFOB_TRY(fbp_group(x, d_sino + (size_t)z * width * height, width, height, nz, d_out + (size_t)z * ow * oh, s));
+        UFOB_TRY(fbp_group(x, plain_rows(d_sino + (size_t)z * width * height, width), width, height, nz,
+                           d_out + (size_t)z * ow * oh, s));
     }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_fbp_run_projections(ufob_fbp *x, const ufob_preprocess *pre, const float *d_proj,
+                                                uint32_t width, uint32_t height, uint32_t n_projections,
+                                                uint32_t first_row, uint32_t n_rows, float *d_out, void *stream)
+{
+    if (!x || !d_proj || !d_out) return fail(UFOB_ERR_INVALID, "fbp_run_projections: NULL argument");
+    UFOB_TRY(ensure_device());
+    if (first_row > height) return fail(UFOB_ERR_INVALID, "fbp: first row %u beyond height %u", first_row, height);
+    if (!n_rows) n_rows = height - first_row;
+    uint32_t ow, oh;
+    UFOB_TRY(ufob_fbp_get_requisition(x, width, n_projections, &ow, &oh));
+    cudaStream_t s = (cudaStream_t)stream;
+    // every slice group reads the same projections: a cone weight restarts at its count each time
+    const uint32_t count0 = pre && pre->cone ? ufob_cone_weight_get_count(pre->cone) : 0;
+    const uint32_t G = group_slices(width, n_projections, n_rows);
+    for (uint32_t z = 0; z < n_rows; z += G) {
+        const uint32_t nz = std::min(G, n_rows - z);
+        if (pre && pre->cone) UFOB_TRY(ufob_cone_weight_set_count(pre->cone, count0));
+        RowSource src;
+        UFOB_TRY(projection_source(pre, d_proj, width, height, n_projections, width, true, first_row + z, nz, src, s));
+        UFOB_TRY(fbp_group(x, src, width, n_projections, nz, d_out + (size_t)z * ow * oh, s));
+    }
+    if (pre && pre->cone) UFOB_TRY(ufob_cone_weight_set_count(pre->cone, count0 + n_projections));
     return UFOB_OK;
 }
 
@@ -750,7 +809,8 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
         UFOB_CUDA_TRY(cudaEventRecord(x->ev_in[b], x->s_copy));
         UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_comp, x->ev_in[b], 0));
         if (c >= 2) UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_comp, x->ev_out[b], 0));  // hout[b] downloaded
-        UFOB_TRY(fbp_group(x, x->hin[b].as<float>(), width, height, nz, x->hout[b].as<float>(), x->s_comp));
+        UFOB_TRY(fbp_group(x, plain_rows(x->hin[b].as<float>(), width), width, height, nz, x->hout[b].as<float>(),
+                           x->s_comp));
         UFOB_CUDA_TRY(cudaEventRecord(x->ev_done[b], x->s_comp));
         UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_d2h, x->ev_done[b], 0));
         UFOB_CUDA_TRY(cudaMemcpyAsync(h_out + (size_t)z * ow * oh, x->hout[b].ptr, (size_t)nz * ow * oh * 4,

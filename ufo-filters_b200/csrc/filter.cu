@@ -287,12 +287,11 @@ __device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
 // and 2*pair+1, or for the slice-quad layout (OUT_F16_QUADS, `P` angles per
 // slice) item pair = (group * P + angle) * 2 + half, i.e. slices
 // 4*group + 2*half and 4*group + 2*half + 1 at one angle.
-template <int OUT>
-__device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32_t width, uint32_t rows,
-                                            uint32_t in_pitch, uint32_t pair, float2 *bufA, float2 *bufB,
-                                            const float2 *tw, const float2 *gains, uint32_t N, int log2N,
-                                            void *__restrict__ out, uint32_t out_w, uint32_t out_pitch,
-                                            uint32_t P = 0)
+template <int OUT, bool PRE>
+__device__ __forceinline__ void filter_pair(const RowSource &src, uint32_t width, uint32_t rows, uint32_t pair,
+                                            float2 *bufA, float2 *bufB, const float2 *tw, const float2 *gains,
+                                            uint32_t N, int log2N, void *__restrict__ out, uint32_t out_w,
+                                            uint32_t out_pitch, uint32_t P = 0)
 {
     uint32_t ra = 2 * pair, rb = 2 * pair + 1, half = 0;
     size_t cell0 = 0;
@@ -307,14 +306,19 @@ __device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32
         cell0 = (size_t)gp * out_pitch;
     }
     const bool hasb = rb < rows;
-    const float *pa = in + (size_t)ra * in_pitch;
-    const float *pb = in + (size_t)rb * in_pitch;
+    uint32_t ya, pa_proj, yb, pb_proj;
+    const float *pa = row_start(src, hasa ? ra : 0, ya, pa_proj);
+    const float *pb = row_start(src, hasb ? rb : 0, yb, pb_proj);
     __syncthreads();  // previous pair's output reads of bufA/bufB (and table loads) are done
     for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
         float a = 0.f, b = 0.f;
-        if (n < width) {
+        if (n < width) {  // zero padding to N comes after the preprocessing
             if (hasa) a = __ldg(pa + n);
             if (hasb) b = __ldg(pb + n);
+            if (PRE) {
+                if (hasa) a = preprocess_value(src, a, n, ya, pa_proj);
+                if (hasb) b = preprocess_value(src, b, n, yb, pb_proj);
+            }
         }
         bufA[n] = make_float2(a, b);
     }
@@ -361,9 +365,8 @@ __device__ __forceinline__ void filter_pair(const float *__restrict__ in, uint32
     }
 }
 
-template <int OUT>
-__global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__restrict__ in, uint32_t width,
-                                                                uint32_t rows, uint32_t in_pitch,
+template <int OUT, bool PRE>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const RowSource src, uint32_t width, uint32_t rows,
                                                                 const float2 *__restrict__ g_tw,
                                                                 const float2 *__restrict__ g_gains, uint32_t N,
                                                                 int log2N, void *__restrict__ out, uint32_t out_w,
@@ -379,7 +382,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const float *__r
     for (uint32_t i = threadIdx.x; i <= N / 2; i += blockDim.x) gains[i] = g_gains[i];
 
     for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x)
-        filter_pair<OUT>(in, width, rows, in_pitch, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch, P);
+        filter_pair<OUT, PRE>(src, width, rows, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch, P);
 }
 
 // Persistent filter stage of an uneven batch: work items (job, row pair) are
@@ -410,79 +413,102 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_batch(const BatchFilt
             for (uint32_t i = threadIdx.x; i <= j.N / 2; i += blockDim.x) gains[i] = j.gains[i];
             loaded = j.tw;
         }
-        filter_pair<OUT>(j.in, j.width, j.rows, j.in_pitch, w.y, bufA, bufB, tw, gains, j.N, j.log2N, j.out, j.out_w,
-                         j.out_pitch);
+        filter_pair<OUT, false>(plain_rows(j.in, j.in_pitch), j.width, j.rows, w.y, bufA, bufB, tw, gains, j.N,
+                                j.log2N, j.out, j.out_w, j.out_pitch);
     }
 }
 
-template <int OUT>
-static ufob_status launch_rows(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
-                               uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s,
-                               uint32_t P = 0)
+template <int OUT, bool PRE>
+static ufob_status launch_rows_t(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                                 void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P)
 {
     const uint32_t N = plan.nfft;
     const size_t smem = sizeof(float2) * (3 * (size_t)N + N / 2 + 1);
-    static bool attr_set[16] = {};
-    int log2N = ilog2(N);
-    if (!attr_set[log2N]) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_filter_rows<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    auto kern = k_filter_rows<OUT, PRE>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)(sizeof(float2) * (3 * (size_t)kMaxFusedFFT + kMaxFusedFFT / 2 + 1))));
-        attr_set[log2N] = true;
+        attr_set = true;
     }
+    const int log2N = ilog2(N);
     int per_sm = 0;
-    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_rows<OUT>, kFilterThreads, smem));
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFilterThreads, smem));
     if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);
     // slice-quad layout: two items per (group of four slices, angle)
     const uint32_t npairs = OUT == OUT_F16_QUADS ? (rows / P + 3) / 4 * P * 2 : (rows + 1) / 2;
     uint32_t grid = (uint32_t)num_sms() * (uint32_t)per_sm * 4;
     if (grid > npairs) grid = npairs;
     if (grid == 0) return UFOB_OK;
-    k_filter_rows<OUT><<<grid, kFilterThreads, smem, s>>>(d_in, width, rows, in_pitch, plan.d_twiddle.as<float2>(),
-                                                          plan.d_gains.as<float2>(), N, log2N, d_out, out_w,
-                                                          out_pitch, npairs, P);
+    kern<<<grid, kFilterThreads, smem, s>>>(src, width, rows, plan.d_twiddle.as<float2>(), plan.d_gains.as<float2>(),
+                                            N, log2N, d_out, out_w, out_pitch, npairs, P);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
 }
 
-ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
-                               uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
-                               uint32_t out_w, uint32_t out_pitch, cudaStream_t stream)
+template <int OUT>
+static ufob_status launch_rows(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                               void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P = 0)
+{
+    if (src.has_pre()) return launch_rows_t<OUT, true>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+    return launch_rows_t<OUT, false>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+}
+
+ufob_status filter_rows_launch_src(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                                   void *d_out, ufob_dtype out_dtype, ufob_layout out_layout, uint32_t out_w,
+                                   uint32_t out_pitch, cudaStream_t stream)
 {
     const uint32_t N = plan.nfft;
     if (N > kMaxFusedFFT || N < 4)
         return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u outside the supported range [4, %u]", N, kMaxFusedFFT);
     if (width > N) return fail(UFOB_ERR_INVALID, "filter: input width %u exceeds FFT width %u", width, N);
     if (out_w > N) return fail(UFOB_ERR_INVALID, "filter: crop width %u exceeds FFT width %u", out_w, N);
-    if (in_pitch < width) return fail(UFOB_ERR_INVALID, "filter: input pitch %u < width %u", in_pitch, width);
     if (out_layout == UFOB_LAYOUT_PAIRS) {
         if (out_pitch < out_w + 1) return fail(UFOB_ERR_INVALID, "filter: pair pitch %u < crop width + 1", out_pitch);
-        if (out_dtype == UFOB_F16) return launch_rows<OUT_F16_PAIRS>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
-        if (out_dtype == UFOB_BF16) return launch_rows<OUT_BF16_PAIRS>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+        if (out_dtype == UFOB_F16) return launch_rows<OUT_F16_PAIRS>(plan, src, width, rows, d_out, out_w, out_pitch, stream);
+        if (out_dtype == UFOB_BF16) return launch_rows<OUT_BF16_PAIRS>(plan, src, width, rows, d_out, out_w, out_pitch, stream);
         return fail(UFOB_ERR_INVALID, "filter: the pair layout needs F16 or BF16 output");
     }
     if (out_pitch < out_w) return fail(UFOB_ERR_INVALID, "filter: output pitch %u < crop width %u", out_pitch, out_w);
     switch (out_dtype) {
-    case UFOB_F32: return launch_rows<OUT_F32>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
-    case UFOB_F16: return launch_rows<OUT_F16>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
-    case UFOB_BF16: return launch_rows<OUT_BF16>(plan, d_in, width, rows, in_pitch, d_out, out_w, out_pitch, stream);
+    case UFOB_F32: return launch_rows<OUT_F32>(plan, src, width, rows, d_out, out_w, out_pitch, stream);
+    case UFOB_F16: return launch_rows<OUT_F16>(plan, src, width, rows, d_out, out_w, out_pitch, stream);
+    case UFOB_BF16: return launch_rows<OUT_BF16>(plan, src, width, rows, d_out, out_w, out_pitch, stream);
     default: return fail(UFOB_ERR_INVALID, "filter: unsupported output dtype %d", (int)out_dtype);
     }
 }
 
+ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t rows,
+                               uint32_t in_pitch, void *d_out, ufob_dtype out_dtype, ufob_layout out_layout,
+                               uint32_t out_w, uint32_t out_pitch, cudaStream_t stream)
+{
+    if (in_pitch < width) return fail(UFOB_ERR_INVALID, "filter: input pitch %u < width %u", in_pitch, width);
+    return filter_rows_launch_src(plan, plain_rows(d_in, in_pitch), width, rows, d_out, out_dtype, out_layout, out_w,
+                                  out_pitch, stream);
+}
+
 // Filter a stack of `nz` sinograms of P rows into the slice-quad FP16 layout
 // ([ceil(nz/4)][P][out_pitch] cells of 16 bytes; see backproject.cu).
-ufob_status filter_quads_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t P, uint32_t nz,
-                                uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch,
-                                cudaStream_t stream)
+ufob_status filter_quads_launch_src(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t P,
+                                    uint32_t nz, void *d_out, uint32_t out_w, uint32_t out_pitch,
+                                    cudaStream_t stream)
 {
     const uint32_t N = plan.nfft;
     if (N > kMaxFusedFFT || N < 4)
         return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u outside the supported range [4, %u]", N, kMaxFusedFFT);
-    if (width > N || out_w > N || in_pitch < width || out_pitch < out_w + 1 || !P)
+    if (width > N || out_w > N || out_pitch < out_w + 1 || !P)
         return fail(UFOB_ERR_INVALID, "filter: bad slice-quad sizes (width %u, N %u, crop %u, pitch %u)", width, N,
                     out_w, out_pitch);
-    return launch_rows<OUT_F16_QUADS>(plan, d_in, width, P * nz, in_pitch, d_out, out_w, out_pitch, stream, P);
+    return launch_rows<OUT_F16_QUADS>(plan, src, width, P * nz, d_out, out_w, out_pitch, stream, P);
+}
+
+ufob_status filter_quads_launch(const FilterPlan &plan, const float *d_in, uint32_t width, uint32_t P, uint32_t nz,
+                                uint32_t in_pitch, void *d_out, uint32_t out_w, uint32_t out_pitch,
+                                cudaStream_t stream)
+{
+    if (in_pitch < width) return fail(UFOB_ERR_INVALID, "filter: input pitch %u < width %u", in_pitch, width);
+    return filter_quads_launch_src(plan, plain_rows(d_in, in_pitch), width, P, nz, d_out, out_w, out_pitch, stream);
 }
 
 // The reference `filter` kernel alone (filter.cl:20-29): out[y][x] = in[y][x] * coeff[x].

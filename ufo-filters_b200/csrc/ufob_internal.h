@@ -81,6 +81,109 @@ ufob_status filter_rows_launch(const FilterPlan &plan, const float *d_in, uint32
 ufob_status filter_spectrum_launch(const float *d_coeff, const float *d_in, float *d_out, uint32_t width2,
                                    uint32_t rows, cudaStream_t stream);
 
+// ---------------------------------------------------------------- preprocessing
+// Per-projection constants of the cone-beam projection weight, computed in FP32
+// on the host the way src/ufo-cone-beam-projection-weight-task.c:128-139 does.
+struct ConeParams {
+    float cx, cz;  // center-position-x/z
+    float mr;      // source / (source + detector distance)
+    float sd;      // source distance
+    float od;      // source + detector distance (source distance when cos(axis-angle-x) ~ 1)
+    float cs;      // cos(axis-angle-x)
+    float pad0, pad1;
+};
+
+// Where logical row r of a row-wise stage comes from.  r = outer * n_inner +
+// inner; the row starts at base + outer * outer_stride + inner * inner_stride
+// floats.  Its (detector row, projection) is (outer, inner) when proj_inner is
+// set (projections read as sinograms) and (inner, outer) otherwise.  Optional
+// per-element steps, applied in the reference's graph order: flat-field
+// correction (src/kernels/ffc.cl:20-50; dark/flat rows of corr_pitch floats
+// indexed by the detector row, or one row for every detector row when
+// corr_pitch is 0) and the cone-beam weight (src/kernels/conebeam.cl:20-36;
+// detector row y0 + y, per-projection constants cone[projection]).
+struct RowSource {
+    const float *base = nullptr;
+    uint64_t outer_stride = 0, inner_stride = 0;
+    uint32_t n_inner = 1, proj_inner = 0;
+    uint32_t y0 = 0;
+    const float *dark = nullptr, *flat = nullptr;
+    uint32_t corr_pitch = 0;
+    float dark_scale = 1.f, flat_scale = 1.f;
+    int absorption = 0, fix_abnormal = 0;
+    const ConeParams *cone = nullptr;
+    bool has_pre() const { return dark != nullptr || cone != nullptr; }
+};
+
+#ifdef __CUDACC__
+#define UFOB_HD __host__ __device__
+#else
+#define UFOB_HD
+#endif
+
+// Rows of `pitch` floats, one after another.
+UFOB_HD inline RowSource plain_rows(const float *base, uint32_t pitch)
+{
+    RowSource s;
+    s.base = base;
+    s.outer_stride = pitch;
+    return s;
+}
+
+#ifdef __CUDACC__
+// Detector row `y` (relative to the dark/flat base) and projection `p` of one
+// row; x = detector column.  FP32 with the reference's operation order, IEEE
+// division and square root.
+__device__ __forceinline__ float preprocess_value(const RowSource &s, float v, uint32_t x, uint32_t y, uint32_t p)
+{
+    if (s.dark) {  // ffc.cl:31-45
+        const size_t i = (size_t)y * s.corr_pitch + x;
+        const float cd = __fmul_rn(__ldg(s.dark + i), s.dark_scale);
+        const float cf = __fmul_rn(__ldg(s.flat + i), s.flat_scale);
+        v = s.absorption ? logf(__fdiv_rn(__fsub_rn(cf, cd), __fsub_rn(v, cd)))
+                         : __fdiv_rn(__fsub_rn(v, cd), __fsub_rn(cf, cd));
+        if (s.fix_abnormal && !isfinite(v)) v = 0.f;
+    }
+    if (s.cone) {  // conebeam.cl:29-35
+        const ConeParams c = s.cone[p];
+        const float fx = __fmul_rn(__fadd_rn(__fsub_rn((float)x, c.cx), 0.5f), c.mr);
+        const float fy = __fmul_rn(__fadd_rn(__fsub_rn((float)(s.y0 + y), c.cz), 0.5f), c.mr);
+        const float den = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.od, c.od), __fmul_rn(fx, fx)), __fmul_rn(fy, fy)));
+        v = __fdiv_rn(__fmul_rn(__fmul_rn(v, c.sd), c.cs), den);
+    }
+    return v;
+}
+
+// Start of logical row r and its (detector row, projection).
+__device__ __forceinline__ const float *row_start(const RowSource &s, uint32_t r, uint32_t &y, uint32_t &p)
+{
+    const uint32_t o = r / s.n_inner, i = r - o * s.n_inner;
+    y = s.proj_inner ? o : i;
+    p = s.proj_inner ? i : o;
+    return s.base + o * s.outer_stride + i * s.inner_stride;
+}
+#endif
+
+// Filter stage over a general row source (see RowSource); rows = logical rows.
+ufob_status filter_rows_launch_src(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                                   void *d_out, ufob_dtype out_dtype, ufob_layout out_layout, uint32_t out_w,
+                                   uint32_t out_pitch, cudaStream_t stream);
+// Slice-quad output of `nz` sinograms of P rows, logical row = slice * P + angle.
+ufob_status filter_quads_launch_src(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t P,
+                                    uint32_t nz, void *d_out, uint32_t out_w, uint32_t out_pitch,
+                                    cudaStream_t stream);
+// RowSource for projections [n][height][pitch]: detector rows first_row ..
+// first_row + n_rows - 1 in projection order (sinograms = false, r = projection
+// * n_rows + row) or as sinograms (true, r = row * n + projection), with the
+// steps of `pre` (its cone weight's count advances by n).
+ufob_status projection_source(const ufob_preprocess *pre, const float *d_proj, uint32_t width, uint32_t height,
+                              uint32_t n, uint32_t pitch, bool sinograms, uint32_t first_row, uint32_t n_rows,
+                              RowSource &src, cudaStream_t s);
+// Row-wise preprocessing alone: logical row r of `src` (width floats) to
+// out + outer * out_outer + inner * out_inner, with the same (outer, inner) split.
+ufob_status rows_pre_launch(const RowSource &src, uint32_t width, uint64_t rows, float *out, uint64_t out_outer,
+                            uint64_t out_inner, cudaStream_t stream);
+
 // ------------------------------------------------------- parallel backprojection
 struct BPGeometry {
     uint32_t W = 0, P = 0, nz = 0;  // sinogram width, rows used, slices

@@ -15,7 +15,7 @@ import math
 import os
 
 __all__ = ["lib", "UfobError", "get_task", "FilterTask", "BackprojectTask", "FBP", "GeneralBackprojectTask",
-           "Batch", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
+           "Batch", "FlatFieldCorrectTask", "ConeBeamProjectionWeightTask", "TransposeProjectionsTask", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libufob.so")
@@ -54,6 +54,16 @@ class Job(ctypes.Structure):
     _fields_ = [("d_sino", ctypes.c_void_p), ("d_out", ctypes.c_void_p), ("width", ctypes.c_uint32),
                 ("height", ctypes.c_uint32), ("axis_pos", ctypes.c_double), ("angle_step", ctypes.c_double),
                 ("angle_offset", ctypes.c_double)]
+
+
+class FFCProps(ctypes.Structure):
+    _fields_ = [("fix_nan_and_inf", ctypes.c_int), ("absorption_correct", ctypes.c_int),
+                ("sinogram_input", ctypes.c_int), ("dark_scale", ctypes.c_float), ("flat_scale", ctypes.c_float)]
+
+
+class Preprocess(ctypes.Structure):
+    _fields_ = [("ffc", ctypes.POINTER(FFCProps)), ("d_dark", ctypes.c_void_p), ("d_flat", ctypes.c_void_p),
+                ("cone", ctypes.c_void_p)]
 
 
 def lib():
@@ -128,6 +138,20 @@ def lib():
             "ufob_cnn_set_step": ([vp, ctypes.c_int64], i),
             "ufob_conv3x3_forward": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "ufob_conv3x3_wgrad": ([vp, vp, vp, i, i, i, i, i, vp], i),
+            "ufob_ffc_props_init": ([ctypes.POINTER(FFCProps)], None),
+            "ufob_ffc_set_property": ([ctypes.POINTER(FFCProps), cs, d], i),
+            "ufob_flat_field_correct": ([ctypes.POINTER(FFCProps), vp, vp, vp, u32, u32, u32, vp, vp], i),
+            "ufob_cone_weight_create": ([ctypes.POINTER(vp)], i),
+            "ufob_cone_weight_set_array": ([vp, cs, vp, u32], i),
+            "ufob_cone_weight_set_property": ([vp, cs, d], i),
+            "ufob_cone_weight_run": ([vp, vp, u32, u32, u32, vp, vp], i),
+            "ufob_cone_weight_set_count": ([vp, u32], i),
+            "ufob_cone_weight_get_count": ([vp], u32),
+            "ufob_cone_weight_destroy": ([vp], None),
+            "ufob_transpose_projections": ([vp, u32, u32, u32, vp, u32, u32, vp], i),
+            "ufob_filter_run_projections": ([vp, ctypes.POINTER(Preprocess), vp, u32, u32, u32, u32, i, u32, u32, vp, i,
+                                             i, u32, vp], i),
+            "ufob_fbp_run_projections": ([vp, ctypes.POINTER(Preprocess), vp, u32, u32, u32, u32, u32, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -264,6 +288,40 @@ class FilterTask(_Task):
         check(lib().ufob_filter_run(self._h, _ptr(sino), W, rows, W, _ptr(out), dt, layout, pitch, _stream(stream)))
         return out
 
+    def process_projections(self, proj, ffc=None, dark=None, flat=None, cone=None, sinograms=True, first_row=0,
+                            n_rows=0, dtype=F32, layout=ROWS, out=None, stream=None):
+        """Filter projections [N, H, W] (float32 CUDA) after flat-field correction
+        (`ffc` a FlatFieldCorrectTask with its dark/flat frames) and/or the cone-beam
+        weight (`cone` a ConeBeamProjectionWeightTask), fused into the filter's loads.
+        sinograms=True: returns the sinograms [n_rows, N, crop] of detector rows
+        first_row.. (QUADS: their slice-quad cells); False: rows in projection order
+        [N, n_rows, crop]."""
+        import torch
+        if proj.dtype != torch.float32 or not proj.is_cuda or proj.dim() != 3:
+            raise ValueError("projections must be a [N, H, W] float32 CUDA tensor")
+        proj = proj.contiguous()
+        N, H, W = proj.shape
+        rows = n_rows or H - first_row
+        cw, _ = self.get_requisition(W, 1)
+        dt = DTYPES.get(dtype, dtype) if isinstance(dtype, str) else dtype
+        pre, keep = _preprocess(ffc, dark, flat, cone)
+        lead = (rows, N) if sinograms else (N, rows)
+        if layout == QUADS:
+            pitch = cw + 1
+            shape = ((rows + 3) // 4, N, pitch, 4)
+            tdt = torch.int32
+        elif layout == PAIRS:
+            pitch = (cw + 1 + 3) // 4 * 4
+            shape, tdt = lead + (pitch,), torch.int32
+        else:
+            pitch = cw
+            shape, tdt = lead + (cw,), {F32: torch.float32, F16: torch.float16, BF16: torch.bfloat16}[dt]
+        out = torch.empty(shape, dtype=tdt, device=proj.device) if out is None else out
+        check(lib().ufob_filter_run_projections(self._h, pre, _ptr(proj), W, H, N, W, int(sinograms), first_row,
+                                                rows, _ptr(out), dt, layout, pitch, _stream(stream)))
+        del keep
+        return out
+
     def apply_spectrum(self, spec, stream=None):
         """The reference ``filter`` task alone on complex-interleaved rows [..., 2*N]."""
         import torch
@@ -371,6 +429,23 @@ class FBP:
         check(lib().ufob_fbp_run(self._h, _ptr(s3), W, H, Z, _ptr(out), _stream(stream)))
         return out[0] if squeeze else out
 
+    def process_projections(self, proj, ffc=None, dark=None, flat=None, first_row=0, n_rows=0, out=None,
+                            stream=None):
+        """``flat-field-correct ! transpose-projections ! fft ! filter ! ifft !
+        backproject`` from projections [N, H, W] (float32 CUDA): one slice per
+        detector row first_row .. first_row + n_rows - 1, [n_rows, roi_h, roi_w]."""
+        import torch
+        proj = proj.contiguous()
+        N, H, W = proj.shape
+        rows = n_rows or H - first_row
+        ow, oh = self.get_requisition(W, N)
+        out = torch.empty((rows, oh, ow), dtype=torch.float32, device=proj.device) if out is None else out
+        pre, keep = _preprocess(ffc, dark, flat, None)
+        check(lib().ufob_fbp_run_projections(self._h, pre, _ptr(proj), W, H, N, first_row, rows, _ptr(out),
+                                             _stream(stream)))
+        del keep
+        return out
+
     def set_timing(self, enable=True):
         check(lib().ufob_fbp_set_timing(self._h, int(enable)))
 
@@ -477,9 +552,156 @@ class Batch:
             self._h = None
 
 
+def _preprocess(ffc, dark, flat, cone):
+    """ctypes Preprocess for the fused filter entry points (None when empty) and
+    the objects it points into, to be kept alive over the call."""
+    if ffc is None and cone is None:
+        return None, ()
+    pre = Preprocess()
+    keep = [pre]
+    if ffc is not None:
+        if dark is None or flat is None:
+            raise ValueError("flat-field correction needs dark and flat")
+        dark, flat = dark.contiguous(), flat.contiguous()
+        pre.ffc = ctypes.pointer(ffc._p)
+        pre.d_dark, pre.d_flat = _ptr(dark), _ptr(flat)
+        keep += [dark, flat, ffc]
+    if cone is not None:
+        pre.cone = cone._h
+        keep.append(cone)
+    return ctypes.byref(pre), keep
+
+
+class FlatFieldCorrectTask:
+    """``flat-field-correct``: (data - dark*ds) / (flat*fs - dark*ds), or with
+    absorption-correct the log of the inverse ratio.
+
+    Properties: fix-nan-and-inf, absorption-correct, sinogram-input,
+    dark-scale, flat-scale (reference defaults)."""
+
+    def __init__(self, **props):
+        self._p = FFCProps()
+        lib().ufob_ffc_props_init(ctypes.byref(self._p))
+        self._values = {}
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def set_property(self, name, value):
+        check(lib().ufob_ffc_set_property(ctypes.byref(self._p), name.encode(), float(value)))
+        self._values[name] = value
+
+    def get_property(self, name):
+        f = {"fix-nan-and-inf": "fix_nan_and_inf", "absorption-correct": "absorption_correct",
+             "sinogram-input": "sinogram_input", "dark-scale": "dark_scale", "flat-scale": "flat_scale"}[name]
+        v = getattr(self._p, f)
+        return bool(v) if isinstance(v, int) else v
+
+    def process(self, data, dark, flat, out=None, stream=None):
+        """data [..., H, W] float32 CUDA; dark/flat [H, W] (or [W] with sinogram-input)."""
+        import torch
+        data, dark, flat = data.contiguous(), dark.contiguous(), flat.contiguous()
+        W = data.shape[-1]
+        H = data.shape[-2] if data.dim() >= 2 else 1
+        n = data.numel() // (W * H)
+        want = (W,) if self._p.sinogram_input else (H, W)
+        if tuple(dark.shape) != want or tuple(flat.shape) != want:
+            raise UfobError(ERR_REQUISITION, "flat-field-correct inputs must have the same size")
+        out = torch.empty_like(data) if out is None else out
+        check(lib().ufob_flat_field_correct(ctypes.byref(self._p), _ptr(data), _ptr(dark), _ptr(flat), W, H, n,
+                                            _ptr(out), _stream(stream)))
+        return out
+
+
+class ConeBeamProjectionWeightTask(_Task):
+    """``cone-beam-projection-weight``.  Array properties center-position-x/z,
+    source-distance, detector-distance (required) and axis-angle-x (default 0);
+    one value broadcasts, else projection i uses value i.  Counts the
+    projections it has weighted, like the task's process()."""
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_cone_weight_create(ctypes.byref(h)))
+        self._h = h
+        self._destroy = L.ufob_cone_weight_destroy
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def set_property(self, name, value):
+        import numpy as np
+        arr = np.ascontiguousarray(np.atleast_1d(np.asarray(value, dtype=np.float64)).reshape(-1))
+        check(lib().ufob_cone_weight_set_array(self._h, name.encode(), arr.ctypes.data, arr.size))
+        self._values[name] = value
+
+    @property
+    def count(self):
+        return int(lib().ufob_cone_weight_get_count(self._h))
+
+    @count.setter
+    def count(self, value):
+        check(lib().ufob_cone_weight_set_count(self._h, int(value)))
+
+    def process(self, proj, out=None, stream=None):
+        """proj [H, W] (one projection) or [n, H, W], float32 CUDA."""
+        import torch
+        proj = proj.contiguous()
+        p3 = proj.unsqueeze(0) if proj.dim() == 2 else proj
+        n, H, W = p3.shape
+        out = torch.empty_like(proj) if out is None else out
+        check(lib().ufob_cone_weight_run(self._h, _ptr(p3), W, H, n, _ptr(out), _stream(stream)))
+        return out
+
+
+class TransposeProjectionsTask:
+    """``transpose-projections`` (a reductor): process() takes projections
+    [H, W] (or [n, H, W]) one after another, generate() then returns the
+    sinograms [num_projections, W] one per call (None at the end).  The
+    sinogram stack lives on the device; `sinograms` is all of it [H, N, W]."""
+
+    def __init__(self, num_projections=0, **props):
+        self.num_projections = int(props.get("num-projections", num_projections))
+        self.sinograms = None
+        self._next = 0
+        self._gen = 0
+
+    def set_property(self, name, value):
+        if name.replace("_", "-") != "num-projections":
+            raise UfobError(ERR_INVALID, "transpose-projections: no property named '%s'" % name)
+        self.num_projections = int(value)
+
+    def get_requisition(self, width, height):
+        return width, self.num_projections
+
+    def process(self, proj, stream=None):
+        """Returns False once num_projections projections were taken (as the task does)."""
+        import torch
+        p3 = (proj.unsqueeze(0) if proj.dim() == 2 else proj).contiguous()
+        n, H, W = p3.shape
+        if self.sinograms is None:
+            if self.num_projections <= 0:
+                raise UfobError(ERR_SETUP, "transpose-projections: num-projections not set")
+            self.sinograms = torch.zeros((H, self.num_projections, W), dtype=torch.float32, device=p3.device)
+        if self._next >= self.num_projections:
+            return False
+        n = min(n, self.num_projections - self._next)
+        check(lib().ufob_transpose_projections(_ptr(p3), W, H, n, _ptr(self.sinograms), self.num_projections,
+                                               self._next, _stream(stream)))
+        self._next += n
+        return True
+
+    def generate(self):
+        if self.sinograms is None or self._gen >= self.sinograms.shape[0]:
+            return None
+        self._gen += 1
+        return self.sinograms[self._gen - 1]
+
+
 def get_task(name, **props):
     """Create a task by its ufo-filters name."""
-    table = {"filter": FilterTask, "backproject": BackprojectTask, "general-backproject": GeneralBackprojectTask}
+    table = {"filter": FilterTask, "backproject": BackprojectTask, "general-backproject": GeneralBackprojectTask,
+             "flat-field-correct": FlatFieldCorrectTask, "cone-beam-projection-weight": ConeBeamProjectionWeightTask,
+             "transpose-projections": TransposeProjectionsTask}
     if name not in table:
         raise KeyError("no task named %r (available: %s)" % (name, ", ".join(sorted(table))))
     return table[name](**props)

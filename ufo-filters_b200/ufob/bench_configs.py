@@ -2,6 +2,7 @@
 
     python -m ufob.bench_configs            # general backprojection and uneven batch
     python -m ufob.bench_configs --gbp      # only the general backprojection
+    python -m ufob.bench_configs --pre      # only the preprocessing stages
 
 * general backprojection: 1024 projections of 1024^2 over 360 degrees into a
   512^3 volume, for the cone geometry (source 800 px before the axis, detector
@@ -13,6 +14,15 @@
   {256, 512, 1024, 1536, 2048} and 180..1800 angles (seeded), filtered and
   backprojected by one persistent launch pair captured in a CUDA graph, for
   FP32 and FP16 filtered storage.
+
+* preprocessing (``--pre``): 1500 raw projections of 256 detector rows x 2048
+  columns with one dark and one flat frame: flat-field correction (with
+  absorption correction) and transpose-projections on their own (GB/s of
+  algorithmic traffic: 4 B read + 4 B written per element), the filter stage
+  fed by them (three passes) against the filter stage with both fused into its
+  loads (one pass), and the whole parallel-beam reconstruction of the 256
+  slices from the raw projections (GUPS) against the same from ready
+  sinograms.
 
 Units are voxel-angle updates per second (GUPS); times come from CUDA events
 after a warm-up call and average over repeated calls.
@@ -85,10 +95,59 @@ def bench_batch(reps=3, seed=2024, jobs=64):
     return out
 
 
+def bench_pre(reps=3, n_proj=1500, rows=256, width=2048, seed=7):
+    import torch
+    from . import F16, FBP, QUADS, FilterTask, FlatFieldCorrectTask, TransposeProjectionsTask
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    dark = 100 + torch.rand(rows, width, device="cuda", generator=g)
+    flat = dark + 1000
+    proj = dark + 900 * torch.rand(n_proj, rows, width, device="cuda", generator=g)
+    ffc = FlatFieldCorrectTask(absorption_correct=1)
+    f = FilterTask()
+    tr = TransposeProjectionsTask(num_projections=n_proj)
+    corrected = ffc.process(proj, dark, flat)
+    tr.process(corrected)
+    sinos = tr.sinograms
+    elems = n_proj * rows * width
+    out = []
+    t_ffc = _timeit(lambda: ffc.process(proj, dark, flat, out=corrected), reps)
+    tr2 = TransposeProjectionsTask(num_projections=n_proj)
+    tr2.sinograms = sinos
+
+    def transpose():
+        tr2._next = 0
+        tr2.process(corrected)
+    t_tr = _timeit(transpose, reps)
+    q = f.process(sinos, dtype=F16, layout=QUADS)
+    t_filt = _timeit(lambda: f.process(sinos, dtype=F16, layout=QUADS, out=q), reps)
+    t_fused = _timeit(lambda: f.process_projections(proj, ffc=ffc, dark=dark, flat=flat, dtype=F16, layout=QUADS,
+                                                    out=q), reps)
+    gb = 8.0 * elems / 1e9
+    out.append({"workload": "flat-field-correct (absorption), %d projections of %dx%d" % (n_proj, rows, width),
+                "ms": round(t_ffc, 3), "gbs": round(gb / t_ffc * 1e3, 1)})
+    out.append({"workload": "transpose-projections, %d projections of %dx%d" % (n_proj, rows, width),
+                "ms": round(t_tr, 3), "gbs": round(gb / t_tr * 1e3, 1)})
+    out.append({"workload": "raw projections -> FP16 slice-quad filtered sinograms (%d x %d x %d)"
+                % (rows, n_proj, width), "separate_ms": round(t_ffc + t_tr + t_filt, 3),
+                "filter_only_ms": round(t_filt, 3), "fused_ms": round(t_fused, 3),
+                "fused_gbs": round(gb / t_fused * 1e3, 1)})
+    del q, corrected
+    fbp = FBP(storage=F16)
+    vol = fbp.process(sinos)
+    t_sino = _timeit(lambda: fbp.process(sinos, out=vol), reps)
+    t_raw = _timeit(lambda: fbp.process_projections(proj, ffc=ffc, dark=dark, flat=flat, out=vol), reps)
+    upd = float(rows) * width * width * n_proj
+    out.append({"workload": "parallel-beam reconstruction of %d slices %d^2 from %d projections, FP16 storage"
+                % (rows, width, n_proj), "from_sinograms_gups": round(upd / t_sino / 1e6, 1),
+                "from_raw_projections_gups": round(upd / t_raw / 1e6, 1)})
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gbp", action="store_true", help="only the general backprojection")
     ap.add_argument("--batch", action="store_true", help="only the uneven batch")
+    ap.add_argument("--pre", action="store_true", help="only the preprocessing stages")
     ap.add_argument("--projections", type=int, default=1024)
     ap.add_argument("--detector", type=int, default=1024)
     ap.add_argument("--volume", type=int, default=512)
@@ -96,10 +155,13 @@ def main(argv=None):
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
-    if not args.batch:
+    only = args.gbp or args.batch or args.pre
+    if args.gbp or not only:
         rows += bench_gbp(args.reps, args.projections, args.detector, args.volume)
-    if not args.gbp:
+    if args.batch or not only:
         rows += bench_batch()
+    if args.pre or not only:
+        rows += bench_pre()
     device_status()
     for r in rows:
         print(json.dumps(r))
