@@ -196,6 +196,28 @@ ufob_status ufob_backproject_run_static(const ufob_bp_props *props, const void *
                                         ufob_layout sino_layout, uint32_t width, uint32_t height, uint32_t nslices,
                                         uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream);
 
+/* ------------------------------------------------------- stacked-backproject
+ * Replaces src/ufo-stacked-backproject-task.c (get_requisition :200-250,
+ * process :302-430, properties :600-690) and src/kernels/stacked-backproject.cl.
+ * Properties: "num-projections", "offset", "axis-pos", "angle-step",
+ * "angle-offset", "roi-x", "roi-y", "roi-width", "roi-height" (as backproject)
+ * and "precision-mode" (0 = int8, 1 = half, 2 = single; default single; nicks
+ * "int8", "half", "single").  Input: a stack of sinograms [nslices][height]
+ * [width] float32; output [nslices][roi_height][roi_width] float32.  The image
+ * orientation is the stacked task's: h = bx cos - by sin + axis.  Unlike the
+ * reference, slices past the last full group of 2 (single) or 4 (half, int8)
+ * are reconstructed too (the reference leaves them unwritten).
+ */
+typedef struct ufob_stacked_bp ufob_stacked_bp;
+ufob_status ufob_stacked_bp_create(ufob_stacked_bp **out);
+ufob_status ufob_stacked_bp_set_property(ufob_stacked_bp *sb, const char *name, double value);
+ufob_status ufob_stacked_bp_set_property_string(ufob_stacked_bp *sb, const char *name, const char *value);
+ufob_status ufob_stacked_bp_get_requisition(ufob_stacked_bp *sb, uint32_t width, uint32_t height,
+                                            uint32_t *out_width, uint32_t *out_height);
+ufob_status ufob_stacked_bp_run(ufob_stacked_bp *sb, const float *d_sino, uint32_t width, uint32_t height,
+                                uint32_t nslices, float *d_out, void *stream);
+void ufob_stacked_bp_destroy(ufob_stacked_bp *sb);
+
 /* ------------------------------------------------------------------- fbp
  * Whole `fft ! filter ! ifft ! backproject` chain for a stack of sinograms
  * [nslices][height][width] float32 -> [nslices][roi_h][roi_w] float32.

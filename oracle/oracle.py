@@ -15,6 +15,8 @@ It restates in NumPy/FP64 what the reference ufo-filters tasks compute:
 * ``backproject`` -- src/ufo-backproject-task.c:96-150,174-267 and
   src/kernels/backproject.cl:24-94 (via the C oracle).
 * ``general_backproject`` -- src/ufo-general-backproject-task.c (via the C oracle).
+* ``stacked_backproject`` -- src/ufo-stacked-backproject-task.c,
+  src/kernels/stacked-backproject.cl (three precision modes).
 * ``flat_field_correct`` -- src/kernels/ffc.cl:20-50 with the task's arguments
   (src/ufo-flat-field-correct-task.c:120-170), in FP32.
 * ``transpose_projections`` -- src/ufo-transpose-projections-task.c:60-120.
@@ -229,6 +231,52 @@ def backproject(sino, num_projections=0, offset=0, axis_pos=-1.0, angle_step=-1.
     lib().oracle_bp_parallel(_p(sino), W, P, nz, _p(s), _p(c), offset, float(np.float32(axis)),
                              roi_x, roi_y, rw, rh, interp, _p(out))
     return out[0] if squeeze else out
+
+
+def stacked_backproject(sino, precision_mode="single", num_projections=0, offset=0, axis_pos=-1.0, angle_step=-1.0,
+                        angle_offset=0.0, roi_x=0, roi_y=0, roi_width=0, roi_height=0):
+    """``stacked-backproject`` (src/ufo-stacked-backproject-task.c:200-430,
+    src/kernels/stacked-backproject.cl) of a stack [Z, P, W] -> FP64 slices.
+    Orientation h = bx cos - by sin + axis (:77); "single" and "half" sample
+    linearly with exact weights and zero outside ("half" after rounding the
+    sinograms to FP16); "int8" quantises with the global min/max, samples the
+    nearest texel floor(h) clamped to the edge, sums integers and dequantises as
+    uninterleave_uint (:360-380), in FP32 like the kernels."""
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    nz, P, W = sino.shape
+    n_proj = num_projections if num_projections else P
+    if P > n_proj or offset + P > n_proj:
+        raise ValueError("sinogram height exceeds num-projections")
+    rw = roi_width if roi_width else W
+    rh = roi_height if roi_height else W
+    axis = axis_pos if axis_pos > 0.0 else float(np.float32(W) / np.float32(2.0))
+    s, c = bp_luts(n_proj, angle_step if angle_step > 0 else 0.0, angle_offset)
+    if precision_mode in ("single", "half"):
+        src = sino if precision_mode == "single" else sino.astype(np.float16).astype(np.float32)
+        out = np.zeros((nz, rh, rw), dtype=np.float64)
+        ms = np.ascontiguousarray(-s)
+        lib().oracle_bp_parallel(_p(np.ascontiguousarray(src)), W, P, nz, _p(ms), _p(c), offset,
+                                 float(np.float32(axis)), roi_x, roi_y, rw, rh, INTERP_EXACT, _p(out))
+        return out
+    if precision_mode != "int8":
+        raise ValueError("precision_mode must be int8, half or single")
+    f32 = np.float32
+    mn, mx = f32(sino.min()), f32(sino.max())
+    scale = f32(f32(255.0) / (mx - mn))
+    q = np.minimum(np.trunc((sino - mn) * scale), 255).astype(np.int64)
+    s32 = s[offset:offset + P].astype(np.float32).astype(np.float64)
+    c32 = c[offset:offset + P].astype(np.float32).astype(np.float64)
+    ax = float(np.float32(axis))
+    bx = (np.arange(rw) + roi_x) - ax + 0.5
+    by = (np.arange(rh) + roi_y) - ax + 0.5
+    sums = np.zeros((nz, rh, rw), dtype=np.int64)
+    for p in range(P):
+        h = bx[None, :] * c32[p] - by[:, None] * s32[p] + ax
+        i = np.clip(np.floor(h).astype(np.int64), 0, W - 1)
+        sums += q[:, p, :][:, i]
+    dq = f32((mx - mn) / f32(255.0))
+    v = (sums.astype(np.float32) * dq + mn).astype(np.float32)
+    return ((v * f32(math.pi)) / f32(P)).astype(np.float64)
 
 
 def fbp(sino, axis_pos=-1.0, size_x=0, crop_width=0, filter_props=None, **bp_props):

@@ -127,3 +127,61 @@ def test_task_table_names():
     assert t.get_requisition(64, 32) == (64, 12)
     with pytest.raises(ufob.UfobError):
         t.set_property("offset", 1)
+
+
+# --------------------------------------------------------------------------- stacked-backproject
+
+def _sino_stack(seed, Z, P, W):
+    ang = np.arange(P) * math.pi / P
+    return np.stack([oracle.ellipse_sinogram(oracle.random_ellipses(seed + z), W, ang) for z in range(Z)])
+
+
+def test_stacked_orientation_is_backproject_flipped():
+    """h = bx cos - by sin + axis: with the default axis W/2 and a full ROI the
+    stacked image is the backproject image mirrored in y (by -> -by)."""
+    s = _sino_stack(3, 2, 60, 48)
+    st = oracle.stacked_backproject(s, "single")
+    bp = oracle.backproject(s)
+    np.testing.assert_allclose(st, bp[:, ::-1, :], rtol=1e-9, atol=1e-9 * np.abs(bp).max())
+
+
+def test_stacked_half_and_int8_modes():
+    s = _sino_stack(4, 3, 90, 64)
+    single = oracle.stacked_backproject(s, "single")
+    half = oracle.stacked_backproject(s, "half")
+    assert oracle.rel_l2(half, single) < 1e-3
+    # int8 on a sinogram whose minimum is 0: the reference's once-added minimum vanishes and the
+    # result is a nearest-neighbour backprojection of 8-bit data (compared inside the inscribed
+    # circle: outside it rays leave the detector, where int8 clamps to the edge and the others read 0)
+    pos = np.maximum(s, 0).astype(np.float32)
+    pos[0, 0, 0] = 0.0
+    roi = dict(roi_x=16, roi_y=16, roi_width=32, roi_height=32)
+    q = oracle.stacked_backproject(pos, "int8", **roi)
+    assert oracle.rel_l2(q, oracle.stacked_backproject(pos, "single", **roi)) < 0.02
+    with pytest.raises(ValueError):
+        oracle.stacked_backproject(s, "double")
+
+
+def test_stacked_int8_dequantisation_formula():
+    """uninterleave_uint adds the minimum once, not once per projection."""
+    P, W = 8, 16
+    s = np.full((1, P, W), 3.0, np.float32)
+    s[0, 0, 0] = 1.0  # min 1, max 3
+    out = oracle.stacked_backproject(s, "int8", roi_x=4, roi_y=4, roi_width=4, roi_height=4)
+    # every sample away from column 0 quantises to 255 -> sum = 255 P
+    expect = (np.float32(255 * P) * np.float32(2.0 / 255.0) + np.float32(1.0)) * np.float32(math.pi) / np.float32(P)
+    np.testing.assert_allclose(out, expect, rtol=1e-6)
+
+
+def test_stacked_task_properties():
+    t = ufob.StackedBackprojectTask(precision_mode="half", axis_pos=10.5)
+    t.set_property("precision-mode", "int8")
+    t.set_property("roi-width", 32)
+    assert t.get_requisition(64, 90) == (32, 64)
+    with pytest.raises(ufob.UfobError):
+        t.set_property("precision-mode", "double")
+    with pytest.raises(ufob.UfobError):
+        t.set_property("mode", "nearest")
+    with pytest.raises(ufob.UfobError):  # more rows than num-projections
+        t.set_property("num-projections", 10)
+        t.get_requisition(64, 90)

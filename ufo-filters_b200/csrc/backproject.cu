@@ -141,20 +141,23 @@ ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, ui
 
 // ------------------------------------------------------------------ sin/cos table
 
-__global__ void k_sincos(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *out)
+// mirror: store -sin, i.e. h = bx cos - by sin + axis (the stacked-backproject orientation,
+// src/kernels/stacked-backproject.cl:77)
+__global__ void k_sincos(double angle_offset, double step, uint32_t lut_offset, uint32_t P, int mirror, float2 *out)
 {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P) return;
     double s, c;
     sincos(angle_offset + (double)(lut_offset + p) * step, &s, &c);  // FP64, cast to FP32 as the reference LUTs
-    out[p] = make_float2((float)s, (float)c);
+    const float fs = (float)s;
+    out[p] = make_float2(mirror ? -fs : fs, (float)c);
 }
 
 ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *d_out,
-                                cudaStream_t stream)
+                                cudaStream_t stream, bool mirror)
 {
     if (!P) return UFOB_OK;
-    k_sincos<<<(P + 255) / 256, 256, 0, stream>>>(angle_offset, step, lut_offset, P, d_out);
+    k_sincos<<<(P + 255) / 256, 256, 0, stream>>>(angle_offset, step, lut_offset, P, mirror ? 1 : 0, d_out);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;

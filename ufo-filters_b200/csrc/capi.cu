@@ -374,6 +374,7 @@ struct ufob_backproject {
     // cache key of the sin/cos table
     uint32_t key_P = 0, key_nproj = 0, key_offset = 0;
     double key_step = 0, key_aoff = 0;
+    bool mirror = false;  // stacked-backproject orientation (-sin table)
 };
 
 extern "C" {
@@ -498,7 +499,7 @@ static ufob_status bp_prepare(ufob_backproject *bp, uint32_t width, uint32_t hei
     if (bp->key_P != height || bp->key_nproj != nproj || bp->key_offset != p.offset || bp->key_step != step ||
         bp->key_aoff != p.angle_offset || !bp->sincos.ptr) {
         UFOB_TRY(bp->sincos.ensure(sizeof(float2) * height));
-        UFOB_TRY(sincos_table_launch(p.angle_offset, step, p.offset, height, bp->sincos.as<float2>(), s));
+        UFOB_TRY(sincos_table_launch(p.angle_offset, step, p.offset, height, bp->sincos.as<float2>(), s, bp->mirror));
         bp->key_P = height;
         bp->key_nproj = nproj;
         bp->key_offset = p.offset;
@@ -647,6 +648,94 @@ extern "C" ufob_status ufob_fbp_get_requisition(ufob_fbp *x, uint32_t width, uin
     uint32_t fw, fh;
     UFOB_TRY(ufob_filter_get_requisition(x->f, width, height, &fw, &fh));
     return ufob_backproject_get_requisition(x->bp, fw, fh, ow, oh);
+}
+
+// ------------------------------------------------------------------ stacked-backproject
+
+struct ufob_stacked_bp {
+    ufob_backproject *bp = nullptr;  // mirrored sine table
+    int precision = 2;               // 0 int8, 1 half, 2 single (src/ufo-stacked-backproject-task.c:705-716)
+    DevBuf work, keys;
+};
+
+extern "C" ufob_status ufob_stacked_bp_create(ufob_stacked_bp **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "stacked_bp_create: out is NULL");
+    ufob_stacked_bp *sb = new ufob_stacked_bp;
+    ufob_status st = ufob_backproject_create(nullptr, &sb->bp);
+    if (st != UFOB_OK) {
+        delete sb;
+        return st;
+    }
+    sb->bp->mirror = true;
+    *out = sb;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_stacked_bp_set_property(ufob_stacked_bp *sb, const char *name, double v)
+{
+    if (!sb) return fail(UFOB_ERR_INVALID, "stacked-backproject handle is NULL");
+    if (prop_is(name, "precision-mode")) {
+        if (!(v == 0 || v == 1 || v == 2)) return fail(UFOB_ERR_INVALID, "stacked-backproject: precision-mode %g", v);
+        sb->precision = (int)v;
+        return UFOB_OK;
+    }
+    if (prop_is(name, "mode") || prop_is(name, "tile") || prop_is(name, "half-sums"))
+        return fail(UFOB_ERR_INVALID, "stacked-backproject: no property named '%s'", name);
+    return ufob_backproject_set_property(sb->bp, name, v);
+}
+
+extern "C" ufob_status ufob_stacked_bp_set_property_string(ufob_stacked_bp *sb, const char *name, const char *value)
+{
+    if (!sb) return fail(UFOB_ERR_INVALID, "stacked-backproject handle is NULL");
+    if (prop_is(name, "precision-mode")) {
+        static const char *nicks[3] = {"int8", "half", "single"};
+        for (int i = 0; i < 3; i++)
+            if (streq(value, nicks[i])) return ufob_stacked_bp_set_property(sb, name, i);
+        return fail(UFOB_ERR_INVALID, "stacked-backproject: unknown precision-mode '%s'", value ? value : "(null)");
+    }
+    char *end = nullptr;
+    double v = value ? strtod(value, &end) : 0.0;
+    if (!value || end == value) return fail(UFOB_ERR_INVALID, "stacked-backproject: '%s' is not a number", value ? value : "(null)");
+    return ufob_stacked_bp_set_property(sb, name, v);
+}
+
+extern "C" ufob_status ufob_stacked_bp_get_requisition(ufob_stacked_bp *sb, uint32_t width, uint32_t height,
+                                                       uint32_t *ow, uint32_t *oh)
+{
+    if (!sb) return fail(UFOB_ERR_INVALID, "stacked-backproject handle is NULL");
+    return ufob_backproject_get_requisition(sb->bp, width, height, ow, oh);
+}
+
+extern "C" ufob_status ufob_stacked_bp_run(ufob_stacked_bp *sb, const float *d_sino, uint32_t width, uint32_t height,
+                                           uint32_t nslices, float *d_out, void *stream)
+{
+    if (!sb || !d_sino || !d_out) return fail(UFOB_ERR_INVALID, "stacked_bp_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!nslices) return UFOB_OK;
+    if (sb->precision == 2)  // single: FP32 rows, linear interpolation
+        return ufob_backproject_run(sb->bp, d_sino, UFOB_F32, UFOB_LAYOUT_ROWS, width, height, nslices, 0, 0, d_out,
+                                    stream);
+    if (sb->precision == 1) {  // half: FP16 slice-quad cells, FP32 sums
+        const uint32_t cells = width + 1;
+        UFOB_TRY(sb->work.ensure((size_t)((nslices + 3) / 4) * height * cells * 16));
+        UFOB_TRY(pack_quads_launch(d_sino, width, height, nslices, sb->work.ptr, s));
+        return ufob_backproject_run(sb->bp, sb->work.ptr, UFOB_F16, UFOB_LAYOUT_QUADS, width, height, nslices, cells,
+                                    (uint64_t)cells * height, d_out, stream);
+    }
+    BPGeometry g;  // int8
+    UFOB_TRY(bp_prepare(sb->bp, width, height, nslices, g, s));
+    UFOB_TRY(sb->work.ensure((size_t)((nslices + 3) / 4) * height * width * 4));
+    UFOB_TRY(sb->keys.ensure(8));
+    return stacked_u8_launch(g, d_sino, sb->work.ptr, sb->keys.as<uint32_t>(), d_out, s);
+}
+
+extern "C" void ufob_stacked_bp_destroy(ufob_stacked_bp *sb)
+{
+    if (!sb) return;
+    ufob_backproject_destroy(sb->bp);
+    delete sb;
 }
 
 // Filter + backproject `nz` slices already on the device; logical row

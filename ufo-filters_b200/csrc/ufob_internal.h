@@ -179,6 +179,13 @@ ufob_status filter_quads_launch_src(const FilterPlan &plan, const RowSource &src
 ufob_status projection_source(const ufob_preprocess *pre, const float *d_proj, uint32_t width, uint32_t height,
                               uint32_t n, uint32_t pitch, bool sinograms, uint32_t first_row, uint32_t n_rows,
                               RowSource &src, cudaStream_t s);
+struct BPGeometry;
+// stacked-backproject helpers: FP32 stack [Z][P][W] -> slice-quad cells
+// [ceil(Z/4)][P][W+1]; the whole int8 path (d_work >= ceil(Z/4)*P*W words,
+// d_keys = 2 words of device scratch).
+ufob_status pack_quads_launch(const float *d_in, uint32_t W, uint32_t P, uint32_t Z, void *d_out, cudaStream_t s);
+ufob_status stacked_u8_launch(const BPGeometry &g, const float *d_sino, void *d_work, uint32_t *d_keys, float *d_out,
+                              cudaStream_t s);
 // Row-wise preprocessing alone: logical row r of `src` (width floats) to
 // out + outer * out_outer + inner * out_inner, with the same (outer, inner) split.
 ufob_status rows_pre_launch(const RowSource &src, uint32_t width, uint64_t rows, float *out, uint64_t out_outer,
@@ -195,7 +202,7 @@ struct BPGeometry {
 
 // sin/cos of angle_offset + (lut_offset + p) * step for p < P, in FP64 on the device.
 ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_offset, uint32_t P, float2 *d_out,
-                                cudaStream_t stream);
+                                cudaStream_t stream, bool mirror = false);
 
 enum SinoKind { SINO_F32 = 0, SINO_F16_PAIRS = 1, SINO_BF16_PAIRS = 2 };
 

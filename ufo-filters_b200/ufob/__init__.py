@@ -15,7 +15,7 @@ import math
 import os
 
 __all__ = ["lib", "UfobError", "get_task", "FilterTask", "BackprojectTask", "FBP", "GeneralBackprojectTask",
-           "Batch", "FlatFieldCorrectTask", "ConeBeamProjectionWeightTask", "TransposeProjectionsTask", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
+           "Batch", "FlatFieldCorrectTask", "ConeBeamProjectionWeightTask", "TransposeProjectionsTask", "StackedBackprojectTask", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libufob.so")
@@ -138,6 +138,12 @@ def lib():
             "ufob_cnn_set_step": ([vp, ctypes.c_int64], i),
             "ufob_conv3x3_forward": ([vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, vp], i),
             "ufob_conv3x3_wgrad": ([vp, vp, vp, i, i, i, i, i, vp], i),
+            "ufob_stacked_bp_create": ([ctypes.POINTER(vp)], i),
+            "ufob_stacked_bp_set_property": ([vp, cs, d], i),
+            "ufob_stacked_bp_set_property_string": ([vp, cs, cs], i),
+            "ufob_stacked_bp_get_requisition": ([vp, u32, u32, pu32, pu32], i),
+            "ufob_stacked_bp_run": ([vp, vp, u32, u32, u32, vp, vp], i),
+            "ufob_stacked_bp_destroy": ([vp], None),
             "ufob_ffc_props_init": ([ctypes.POINTER(FFCProps)], None),
             "ufob_ffc_set_property": ([ctypes.POINTER(FFCProps), cs, d], i),
             "ufob_flat_field_correct": ([ctypes.POINTER(FFCProps), vp, vp, vp, u32, u32, u32, vp, vp], i),
@@ -552,6 +558,43 @@ class Batch:
             self._h = None
 
 
+class StackedBackprojectTask(_Task):
+    """``stacked-backproject``: a stack of sinograms [Z, P, W] -> [Z, roi_h, roi_w]
+    with the task's orientation (h = bx cos - by sin + axis).
+
+    Properties: num-projections, offset, axis-pos, angle-step, angle-offset,
+    roi-x/y/width/height and precision-mode ("int8", "half", "single")."""
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_stacked_bp_create(ctypes.byref(h)))
+        self._h = h
+        self._set_num, self._set_str, self._destroy = (L.ufob_stacked_bp_set_property,
+                                                       L.ufob_stacked_bp_set_property_string,
+                                                       L.ufob_stacked_bp_destroy)
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def get_requisition(self, width, height):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_stacked_bp_get_requisition(self._h, width, height, ctypes.byref(w), ctypes.byref(h)))
+        return w.value, h.value
+
+    def process(self, sino, out=None, stream=None):
+        import torch
+        if sino.dtype != torch.float32 or not sino.is_cuda:
+            raise ValueError("sinograms must be a float32 CUDA tensor")
+        squeeze = sino.dim() == 2
+        s3 = (sino.unsqueeze(0) if squeeze else sino).contiguous()
+        Z, H, W = s3.shape
+        ow, oh = self.get_requisition(W, H)
+        out = torch.empty((Z, oh, ow), dtype=torch.float32, device=s3.device) if out is None else out
+        check(lib().ufob_stacked_bp_run(self._h, _ptr(s3), W, H, Z, _ptr(out), _stream(stream)))
+        return out[0] if squeeze else out
+
+
 def _preprocess(ffc, dark, flat, cone):
     """ctypes Preprocess for the fused filter entry points (None when empty) and
     the objects it points into, to be kept alive over the call."""
@@ -701,7 +744,7 @@ def get_task(name, **props):
     """Create a task by its ufo-filters name."""
     table = {"filter": FilterTask, "backproject": BackprojectTask, "general-backproject": GeneralBackprojectTask,
              "flat-field-correct": FlatFieldCorrectTask, "cone-beam-projection-weight": ConeBeamProjectionWeightTask,
-             "transpose-projections": TransposeProjectionsTask}
+             "transpose-projections": TransposeProjectionsTask, "stacked-backproject": StackedBackprojectTask}
     if name not in table:
         raise KeyError("no task named %r (available: %s)" % (name, ", ".join(sorted(table))))
     return table[name](**props)

@@ -3,6 +3,7 @@
     python -m ufob.bench_configs            # general backprojection and uneven batch
     python -m ufob.bench_configs --gbp      # only the general backprojection
     python -m ufob.bench_configs --pre      # only the preprocessing stages
+    python -m ufob.bench_configs --stacked  # only stacked-backproject
 
 * general backprojection: 1024 projections of 1024^2 over 360 degrees into a
   512^3 volume, for the cone geometry (source 800 px before the axis, detector
@@ -23,6 +24,9 @@
   loads (one pass), and the whole parallel-beam reconstruction of the 256
   slices from the raw projections (GUPS) against the same from ready
   sinograms.
+
+* stacked-backproject (``--stacked``): 32 slices of 2048^2 from 1500 angles
+  (uniform random sinograms) in the three precision modes.
 
 Units are voxel-angle updates per second (GUPS); times come from CUDA events
 after a warm-up call and average over repeated calls.
@@ -143,11 +147,28 @@ def bench_pre(reps=3, n_proj=1500, rows=256, width=2048, seed=7):
     return out
 
 
+def bench_stacked(reps=2, Z=32, P=1500, W=2048, seed=11):
+    """stacked-backproject in its three precision modes on Z slices of W^2 from P angles."""
+    import torch
+    from . import StackedBackprojectTask
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    sino = torch.rand(Z, P, W, device="cuda", generator=g) - 0.5
+    out = torch.empty(Z, W, W, device="cuda")
+    rows = []
+    for mode in ("single", "half", "int8"):
+        t = StackedBackprojectTask(precision_mode=mode)
+        ms = _timeit(lambda: t.process(sino, out=out), reps)
+        rows.append({"workload": "stacked-backproject precision-mode=%s, %d slices %d^2 from %d angles"
+                     % (mode, Z, W, P), "ms": round(ms, 2), "gups": round(float(Z) * W * W * P / ms / 1e6, 1)})
+    return rows
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gbp", action="store_true", help="only the general backprojection")
     ap.add_argument("--batch", action="store_true", help="only the uneven batch")
     ap.add_argument("--pre", action="store_true", help="only the preprocessing stages")
+    ap.add_argument("--stacked", action="store_true", help="only stacked-backproject")
     ap.add_argument("--projections", type=int, default=1024)
     ap.add_argument("--detector", type=int, default=1024)
     ap.add_argument("--volume", type=int, default=512)
@@ -155,13 +176,15 @@ def main(argv=None):
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
-    only = args.gbp or args.batch or args.pre
+    only = args.gbp or args.batch or args.pre or args.stacked
     if args.gbp or not only:
         rows += bench_gbp(args.reps, args.projections, args.detector, args.volume)
     if args.batch or not only:
         rows += bench_batch()
     if args.pre or not only:
         rows += bench_pre()
+    if args.stacked or not only:
+        rows += bench_stacked()
     device_status()
     for r in rows:
         print(json.dumps(r))
