@@ -274,6 +274,39 @@ ufob_status ufob_gbp_process(ufob_gbp *g, const float *d_projection, uint32_t wi
 ufob_status ufob_gbp_generate(ufob_gbp *g, void *d_slice, uint32_t index, void *stream);
 void ufob_gbp_destroy(ufob_gbp *g);
 
+/* ------------------------------------------------------- lamino-backproject
+ * Replaces src/ufo-lamino-backproject-task.c (setup :164-237, get_requisition
+ * :239-256, process :280-500, generate :502-517, properties :690-811) and the
+ * kernels generated from src/kernels/templates/{z,center,lamino,roll}_template.in.
+ * Numeric properties: "z", "num-projections", "overall-angle" (default pi),
+ * "tomo-angle" (default unset: overall-angle * i / num-projections for
+ * projection i), "lamino-angle", "roll-angle", "parameter" (0 z, 1 x-center,
+ * 2 lamino-angle, 3 roll-angle; nicks "z", "x-center", "lamino-angle",
+ * "roll-angle").  Array properties (ufob_lamino_set_array): "x-region",
+ * "y-region" (3 integers from, to, step), "region" (3 floats: the swept
+ * parameter), "projection-offset" (2 integers), "center" (2 floats).  String
+ * property "addressing-mode" ("clamp" default, "clamp_to_edge", "none").
+ * Output: [nz][ny][nx] float32, nx = (to - from - 1) / step + 1 of x-region
+ * (likewise ny), nz = ceil((region.to - region.from) / region.step).
+ */
+typedef struct ufob_lamino ufob_lamino;
+ufob_status ufob_lamino_create(ufob_lamino **out);
+ufob_status ufob_lamino_set_property(ufob_lamino *l, const char *name, double value);
+ufob_status ufob_lamino_set_property_string(ufob_lamino *l, const char *name, const char *value);
+ufob_status ufob_lamino_set_array(ufob_lamino *l, const char *name, const double *values, uint32_t n);
+ufob_status ufob_lamino_setup(ufob_lamino *l);
+ufob_status ufob_lamino_get_requisition(ufob_lamino *l, uint32_t *nx, uint32_t *ny, uint32_t *nz);
+/* All num-projections projections [n][height][width] at once (projection i is
+ * the task's i-th process() call) -> the volume. */
+ufob_status ufob_lamino_run(ufob_lamino *l, const float *d_proj, uint32_t width, uint32_t height, float *d_volume,
+                            void *stream);
+/* Streaming form of the reductor: process() per projection, then one
+ * generate() of the whole volume (fails before all projections arrived). */
+ufob_status ufob_lamino_process(ufob_lamino *l, const float *d_projection, uint32_t width, uint32_t height,
+                                void *stream);
+ufob_status ufob_lamino_generate(ufob_lamino *l, float *d_volume, void *stream);
+void ufob_lamino_destroy(ufob_lamino *l);
+
 /* ------------------------------------------------------------ batched jobs
  * Uneven batch of parallel-beam reconstructions run by one persistent kernel
  * over a device work queue (captured in a CUDA graph on first use).

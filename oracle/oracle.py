@@ -17,6 +17,8 @@ It restates in NumPy/FP64 what the reference ufo-filters tasks compute:
 * ``general_backproject`` -- src/ufo-general-backproject-task.c (via the C oracle).
 * ``stacked_backproject`` -- src/ufo-stacked-backproject-task.c,
   src/kernels/stacked-backproject.cl (three precision modes).
+* ``lamino_backproject`` -- src/ufo-lamino-backproject-task.c and the kernels
+  generated from src/kernels/templates/*_template.in.
 * ``flat_field_correct`` -- src/kernels/ffc.cl:20-50 with the task's arguments
   (src/ufo-flat-field-correct-task.c:120-170), in FP32.
 * ``transpose_projections`` -- src/ufo-transpose-projections-task.c:60-120.
@@ -382,6 +384,84 @@ def general_backproject(proj, num_projections, region=(0.0, 0.0, 0.0), x_region=
     out = np.zeros((nz, ny, nx), dtype=np.float64)
     lib().oracle_gbp(_p(proj), W, H, n, _p(table), flags, param_col, _p(slice_values), float(z),
                      x0, dx, y0, dy, nx, ny, nz, norm, interp, addr, _p(out))
+    return out
+
+
+def _bilinear(img, u, v, addressing_mode="clamp"):
+    """Linear sample of img [H, W] at unnormalised (u, v), texel centres at +1/2;
+    outside the image 0 ("clamp") or the edge texel ("clamp_to_edge", "none")."""
+    H, W = img.shape
+    x, y = u - 0.5, v - 0.5
+    i0, j0 = np.floor(x).astype(np.int64), np.floor(y).astype(np.int64)
+    a, b = x - i0, y - j0
+
+    def fetch(i, j):
+        if addressing_mode == "clamp":
+            ok = (i >= 0) & (i < W) & (j >= 0) & (j < H)
+            return np.where(ok, img[np.clip(j, 0, H - 1), np.clip(i, 0, W - 1)], 0.0)
+        return img[np.clip(j, 0, H - 1), np.clip(i, 0, W - 1)]
+    return ((1 - a) * (1 - b) * fetch(i0, j0) + a * (1 - b) * fetch(i0 + 1, j0) + (1 - a) * b * fetch(i0, j0 + 1)
+            + a * b * fetch(i0 + 1, j0 + 1))
+
+
+def lamino_backproject(proj, num_projections, x_region, y_region, region, z=0.0, projection_offset=(0, 0),
+                       center=(0.0, 0.0), overall_angle=math.pi, tomo_angle=None, lamino_angle=0.0, roll_angle=0.0,
+                       parameter="z", addressing_mode="clamp"):
+    """``lamino-backproject`` of projections [n, H, W] -> FP64 volume [nz, ny, nx].
+
+    src/ufo-lamino-backproject-task.c:239-256 (sizes), :280-360 (the FP32
+    scalars, formed here the same way) and the generated kernels
+    (src/kernels/templates/{z,center,lamino,roll}_template.in, definitions.in:
+    rotate() updates pixel.x before it enters pixel.y, as written there)."""
+    f32 = np.float32
+    proj = np.asarray(proj, dtype=np.float64)
+    n = num_projections
+    if proj.shape[0] != n:
+        raise ValueError("need num-projections projections")
+    size = lambda r: 0 if r[2] == 0 else max(0, int((r[1] - r[0] - 1) / r[2]) + 1)  # C integer division
+    nx, ny = size([int(t) for t in x_region]), size([int(t) for t in y_region])
+    reg = [f32(t) for t in region]
+    nz = int(math.ceil(f32((reg[1] - reg[0]) / reg[2])))
+    norm = float(f32(abs(float(f32(overall_angle))) / n))
+    xs, x0 = float(int(x_region[2])), float(int(x_region[0]))
+    ys, y0 = float(int(y_region[2])), float(int(y_region[0]))
+    px_off, py_off = int(projection_offset[0]), int(projection_offset[1])
+    if parameter == "x-center":
+        xc0, xcs = float(f32(reg[0] - f32(px_off))), float(reg[2])
+    else:
+        xc0 = float(f32(f32(center[0]) - f32(px_off)))
+        xcs = xc0
+    yc = float(f32(f32(center[1]) - f32(py_off)))
+    ix, iy = np.meshgrid(np.arange(nx, dtype=np.float64), np.arange(ny, dtype=np.float64))
+    vx, vy = ix * xs + x0, iy * ys + y0
+    out = np.zeros((nz, ny, nx))
+    ov = f32(overall_angle)
+    for k in range(nz):
+        vz = float(f32(f32(k) * reg[2] + reg[0])) if parameter == "z" else float(f32(z))
+        la = f32(lamino_angle)
+        sL, cL = float(f32(math.sin(la))), float(f32(math.cos(la)))
+        ra = f32(-f32(roll_angle))
+        sR, cR = float(f32(math.sin(ra))), float(f32(math.cos(ra)))
+        xcc = xc0
+        if parameter == "x-center":
+            xcc = float(f32(f32(k) * f32(xcs) + f32(xc0)))
+        elif parameter == "lamino-angle":
+            a = f32(f32(k) * reg[2] + reg[0])
+            sL, cL = float(f32(math.sin(a))), float(f32(math.cos(a)))
+        elif parameter == "roll-angle":
+            a = f32(f32(k) * -reg[2] - reg[0])
+            sR, cR = float(f32(math.sin(a))), float(f32(math.cos(a)))
+        acc = np.zeros((ny, nx))
+        for p in range(n):
+            t = f32(tomo_angle) if tomo_angle is not None else f32(f32(ov * f32(p)) / f32(n))
+            sn, cs = float(f32(math.sin(t))), float(f32(math.cos(t)))
+            px = vx * cs + vy * sn + xcc
+            py = (vx * cL) * sn + (-vy * cL) * cs + (vz * sL + yc)
+            a1, b1 = px - xc0, py - yc
+            a2 = a1 * cR + b1 * sR
+            b2 = -a2 * sR + b1 * cR
+            acc += _bilinear(proj[p], a2 + xc0, b2 + yc, addressing_mode)
+        out[k] = acc * norm
     return out
 
 

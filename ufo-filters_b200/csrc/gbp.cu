@@ -30,6 +30,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <string>
 
@@ -914,3 +915,276 @@ extern "C" ufob_status ufob_gbp_generate(ufob_gbp *g, void *d_slice, uint32_t in
 }
 
 extern "C" void ufob_gbp_destroy(ufob_gbp *g) { delete g; }
+
+// ------------------------------------------------------------------ lamino-backproject
+//
+// src/ufo-lamino-backproject-task.c (setup :164-237, get_requisition :239-256,
+// process :280-500, properties :690-811) with the kernels generated from
+// src/kernels/templates/{z,center,lamino,roll}_template.in, common.in and
+// definitions.in.  Per voxel (idx, idy, idz) and projection (sin, cos of the
+// tomographic angle):
+//   vx = idx * x_step + x_from, vy = idy * y_step + y_from, vz = z (or the z region)
+//   px = vx cos + vy sin + xc                     (xc per slice for parameter x-center)
+//   py = (vx cosL) sin + (-vy cosL) cos + vz sinL + yc
+//   rotate(): px -= xc0; py -= yc; px = px cosR + py sinR; py = -px sinR + py cosR
+//             (the updated px enters the second line); px += xc0; py += yc
+//   volume += norm * sample(px, py)    (linear, texel centres at +1/2)
+// with sin/cos of the lamino angle per slice for parameter lamino-angle and of
+// minus the roll angle per slice for parameter roll-angle.  Every step is
+// affine in (idx, idy, vz), so each (slice, projection) becomes one table of
+// the general backprojector (k_gbp, FP32 texture gathers, exact weights); the
+// FP32 scalars are formed as the task forms them on the host.
+
+struct ufob_lamino {
+    int x_region[3] = {0, 0, 0}, y_region[3] = {0, 0, 0};  // (from, to, step), integers
+    float region[3] = {0.f, 0.f, 0.f};
+    float z = 0.f;
+    int projection_offset[2] = {0, 0};
+    float center[2] = {0.f, 0.f};
+    uint32_t num_projections = 0;
+    float overall_angle = (float)M_PI;
+    float tomo_angle = -FLT_MAX;
+    float lamino_angle = 0.f, roll_angle = 0.f;
+    int parameter = 0;  // z, x-center, lamino-angle, roll-angle
+    int addressing_mode = AD_CLAMP;
+    ufob_gbp g;  // tables, textures
+    uint32_t pushed = 0, pw = 0, ph = 0;
+    bool generated = false;
+    DevBuf d_proj;
+};
+
+namespace {
+const char *kLaminoParams[] = {"z", "x-center", "lamino-angle", "roll-angle"};
+
+uint32_t lamino_region_size(const int r[3])
+{
+    // REGION_SIZE, src/ufo-lamino-backproject-task.c:41-43 (integer arithmetic)
+    return r[2] == 0 ? 0u : (uint32_t)std::max(0, (r[1] - r[0] - 1) / r[2] + 1);
+}
+}  // namespace
+
+extern "C" ufob_status ufob_lamino_create(ufob_lamino **out)
+{
+    if (!out) return fail(UFOB_ERR_INVALID, "lamino_create: out is NULL");
+    *out = new ufob_lamino;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_lamino_set_array(ufob_lamino *l, const char *name, const double *v, uint32_t n)
+{
+    if (!l || (!v && n)) return fail(UFOB_ERR_INVALID, "lamino_set_array: NULL argument");
+    if (name_is(name, "x-region") || name_is(name, "y-region")) {
+        if (n != 3) return fail(UFOB_ERR_INVALID, "%s needs 3 values (from, to, step)", name);
+        // set_region (:110-123): from > to is refused with a warning and the old value kept
+        if ((int)v[0] > (int)v[1]) return UFOB_OK;
+        int *r = name_is(name, "x-region") ? l->x_region : l->y_region;
+        for (int i = 0; i < 3; i++) r[i] = (int)v[i];
+    } else if (name_is(name, "region")) {
+        if (n != 3) return fail(UFOB_ERR_INVALID, "region needs 3 values (from, to, step)");
+        for (int i = 0; i < 3; i++) l->region[i] = (float)v[i];
+    } else if (name_is(name, "projection-offset")) {
+        if (n != 2) return fail(UFOB_ERR_INVALID, "projection-offset needs 2 values");
+        for (int i = 0; i < 2; i++) l->projection_offset[i] = (int)v[i];
+    } else if (name_is(name, "center")) {
+        if (n != 2) return fail(UFOB_ERR_INVALID, "center needs 2 values (x, y)");
+        for (int i = 0; i < 2; i++) l->center[i] = (float)v[i];
+    } else {
+        return fail(UFOB_ERR_INVALID, "lamino-backproject: no array property named '%s'", name ? name : "(null)");
+    }
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_lamino_set_property(ufob_lamino *l, const char *name, double v)
+{
+    if (!l) return fail(UFOB_ERR_INVALID, "lamino handle is NULL");
+    if (name_is(name, "z")) l->z = (float)v;
+    else if (name_is(name, "num-projections")) {
+        if (v < 0 || v > 32768) return fail(UFOB_ERR_INVALID, "num-projections outside [0, 32768]");
+        l->num_projections = (uint32_t)v;
+    } else if (name_is(name, "overall-angle")) l->overall_angle = (float)v;
+    else if (name_is(name, "tomo-angle")) l->tomo_angle = (float)v;
+    else if (name_is(name, "lamino-angle")) l->lamino_angle = (float)v;
+    else if (name_is(name, "roll-angle")) l->roll_angle = (float)v;
+    else if (name_is(name, "parameter")) {
+        if (!(v >= 0 && v <= 3)) return fail(UFOB_ERR_INVALID, "parameter %g", v);
+        l->parameter = (int)v;
+    } else return fail(UFOB_ERR_INVALID, "lamino-backproject: no numeric property named '%s'", name ? name : "(null)");
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_lamino_set_property_string(ufob_lamino *l, const char *name, const char *value)
+{
+    if (!l) return fail(UFOB_ERR_INVALID, "lamino handle is NULL");
+    int i;
+    if (name_is(name, "parameter")) {
+        if ((i = lookup(value, kLaminoParams, 4)) < 0) return fail(UFOB_ERR_INVALID, "unknown parameter '%s'", value);
+        l->parameter = i;
+        return UFOB_OK;
+    }
+    if (name_is(name, "addressing-mode")) {
+        if ((i = lookup(value, kAddrNames, 5)) < 0) return fail(UFOB_ERR_INVALID, "unknown addressing-mode '%s'", value);
+        l->addressing_mode = i;
+        return UFOB_OK;
+    }
+    char *end = nullptr;
+    double v = value ? strtod(value, &end) : 0.0;
+    if (!value || end == value) return fail(UFOB_ERR_INVALID, "'%s' is not a number", value ? value : "(null)");
+    return ufob_lamino_set_property(l, name, v);
+}
+
+extern "C" ufob_status ufob_lamino_setup(ufob_lamino *l)
+{
+    if (!l) return fail(UFOB_ERR_INVALID, "lamino handle is NULL");
+    if (!l->num_projections) return fail(UFOB_ERR_SETUP, "Number of projections has not been set");
+    if (l->region[2] == 0.0f) return fail(UFOB_ERR_SETUP, "Step in region is 0");
+    if (l->addressing_mode == AD_REPEAT || l->addressing_mode == AD_MIRRORED_REPEAT)
+        return fail(UFOB_ERR_UNSUPPORTED, "addressing-mode %s is undefined for unnormalised coordinates",
+                    kAddrNames[l->addressing_mode]);
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_lamino_get_requisition(ufob_lamino *l, uint32_t *nx, uint32_t *ny, uint32_t *nz)
+{
+    if (!l) return fail(UFOB_ERR_INVALID, "lamino handle is NULL");
+    const uint32_t x = lamino_region_size(l->x_region), y = lamino_region_size(l->y_region);
+    const float n = ceilf((l->region[1] - l->region[0]) / l->region[2]);
+    const uint32_t z = l->region[2] == 0.0f || !(n > 0) ? 0u : (uint32_t)n;
+    if (nx) *nx = x;
+    if (ny) *ny = y;
+    if (nz) *nz = z;
+    return UFOB_OK;
+}
+
+static ufob_status lamino_compute(ufob_lamino *l, const float *d_proj, uint32_t W, uint32_t H, float *d_vol,
+                                  cudaStream_t s)
+{
+    UFOB_TRY(ufob_lamino_setup(l));
+    uint32_t nx, ny, nz;
+    UFOB_TRY(ufob_lamino_get_requisition(l, &nx, &ny, &nz));
+    if (!nx || !ny || !nz) return fail(UFOB_ERR_REQUISITION, "lamino-backproject: empty output region");
+    const uint32_t n = l->num_projections;
+    const int par = l->parameter;
+    const bool paramz = par == 0;
+    const uint32_t tab_slices = paramz ? 1 : nz;
+    // FP32 scalars as the task forms them (process :300-360)
+    const float norm = (float)(fabs((double)l->overall_angle) / n);
+    const float xs = (float)l->x_region[2], x0 = (float)l->x_region[0];
+    const float ys = (float)l->y_region[2], y0 = (float)l->y_region[0];
+    const float xc0 = par == 1 ? l->region[0] - (float)l->projection_offset[0]
+                               : l->center[0] - (float)l->projection_offset[0];
+    const float xcs = par == 1 ? l->region[2] : xc0;
+    const float yc = l->center[1] - (float)l->projection_offset[1];
+    std::vector<double> zvals(nz);
+    for (uint32_t k = 0; k < nz; k++)
+        zvals[k] = paramz ? (double)fmaf((float)k, l->region[2], l->region[0]) : (double)l->z;
+    std::vector<float> tab((size_t)tab_slices * n * kTab, 0.0f);
+    for (uint32_t sl = 0; sl < tab_slices; sl++) {
+        float sinL = sinf(l->lamino_angle), cosL = cosf(l->lamino_angle);
+        float sinR = sinf(-l->roll_angle), cosR = cosf(-l->roll_angle);
+        float xcc = xc0;
+        if (par == 1) xcc = fmaf((float)sl, xcs, xc0);
+        if (par == 2) {
+            const float a = fmaf((float)sl, l->region[2], l->region[0]);
+            sinL = sinf(a);
+            cosL = cosf(a);
+        }
+        if (par == 3) {
+            const float a = fmaf((float)sl, -l->region[2], -l->region[0]);
+            sinR = sinf(a);
+            cosR = cosf(a);
+        }
+        for (uint32_t p = 0; p < n; p++) {
+            const float t = l->tomo_angle > -FLT_MAX ? l->tomo_angle : l->overall_angle * (float)p / (float)n;
+            const double sn = (double)(float)sin((double)t), cs = (double)(float)cos((double)t);
+            // rows over X = (idx, idy, vz, 1)
+            const double VX[4] = {xs, 0.0, 0.0, x0}, VY[4] = {0.0, ys, 0.0, y0}, VZ[4] = {0.0, 0.0, 1.0, 0.0};
+            double px[4], py[4], u[4], v[4];
+            for (int i = 0; i < 4; i++) {
+                px[i] = VX[i] * cs + VY[i] * sn + (i == 3 ? (double)xcc : 0.0);
+                py[i] = VX[i] * (double)cosL * sn - VY[i] * (double)cosL * cs + VZ[i] * (double)sinL +
+                        (i == 3 ? (double)yc : 0.0);
+            }
+            for (int i = 0; i < 4; i++) {  // rotate() with its sequential update
+                const double a = px[i] - (i == 3 ? (double)xc0 : 0.0), b = py[i] - (i == 3 ? (double)yc : 0.0);
+                const double a2 = a * cosR + b * sinR;
+                const double b2 = -a2 * sinR + b * cosR;
+                u[i] = a2 + (i == 3 ? (double)xc0 : 0.0);
+                v[i] = b2 + (i == 3 ? (double)yc : 0.0);
+            }
+            float *e = &tab[((size_t)sl * n + p) * kTab];
+            for (int i = 0; i < 4; i++) {
+                e[i] = (float)u[i];
+                e[4 + i] = (float)v[i];
+            }
+        }
+    }
+    ufob_gbp &g = l->g;
+    UFOB_TRY(g.d_tab_f.ensure(tab.size() * sizeof(float)));
+    UFOB_TRY(g.d_zvals.ensure(nz * sizeof(double)));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(g.d_tab_f.ptr, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    UFOB_CUDA_TRY(cudaMemcpyAsync(g.d_zvals.ptr, zvals.data(), nz * sizeof(double), cudaMemcpyHostToDevice, s));
+    // the host vectors must outlive the copies: pageable sources are staged before the calls return
+    GBPArgs a;
+    a.proj = d_proj;
+    a.W = W;
+    a.H = H;
+    a.n_proj = n;
+    a.nx = nx;
+    a.ny = ny;
+    a.nz = nz;
+    a.burst = 16;  // BURST, meson option lamino_backproject_burst_mode (default 16)
+    a.tab = g.d_tab_f.ptr;
+    a.zvals = g.d_zvals.as<double>();
+    a.norm = norm;
+    a.sp.kind = ST_FLOAT;
+    a.sp.gray_min = 0.0;
+    a.sp.maxval = 0.0;
+    a.sp.gray_scale = 0.0;
+    a.addr = l->addressing_mode == AD_CLAMP ? AD_CLAMP : AD_CLAMP_TO_EDGE;
+    a.vol = d_vol;
+    a.tex = nullptr;
+    if (gbp_textures(&g, d_proj, W, H, n, a.addr, s)) a.tex = g.d_tex.as<cudaTextureObject_t>();
+    return launch_gbp_rt<false, float>(a, RT_FLOAT, paramz, s);
+}
+
+extern "C" ufob_status ufob_lamino_run(ufob_lamino *l, const float *d_proj, uint32_t W, uint32_t H, float *d_vol,
+                                       void *stream)
+{
+    if (!l || !d_proj || !d_vol) return fail(UFOB_ERR_INVALID, "lamino_run: NULL argument");
+    UFOB_TRY(ensure_device());
+    return lamino_compute(l, d_proj, W, H, d_vol, (cudaStream_t)stream);
+}
+
+extern "C" ufob_status ufob_lamino_process(ufob_lamino *l, const float *d_projection, uint32_t W, uint32_t H,
+                                           void *stream)
+{
+    if (!l || !d_projection) return fail(UFOB_ERR_INVALID, "lamino_process: NULL argument");
+    UFOB_TRY(ensure_device());
+    UFOB_TRY(ufob_lamino_setup(l));
+    if (l->pushed == 0) {
+        l->pw = W;
+        l->ph = H;
+        UFOB_TRY(l->d_proj.ensure((size_t)l->num_projections * W * H * sizeof(float)));
+    }
+    if (W != l->pw || H != l->ph) return fail(UFOB_ERR_INVALID, "projection size changed within the stream");
+    if (l->pushed >= l->num_projections)
+        return fail(UFOB_ERR_INVALID, "received more than num-projections (%u) projections", l->num_projections);
+    UFOB_CUDA_TRY(cudaMemcpyAsync(l->d_proj.as<float>() + (size_t)l->pushed * W * H, d_projection,
+                                  (size_t)W * H * sizeof(float), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    l->pushed++;
+    return UFOB_OK;
+}
+
+extern "C" ufob_status ufob_lamino_generate(ufob_lamino *l, float *d_vol, void *stream)
+{
+    if (!l || !d_vol) return fail(UFOB_ERR_INVALID, "lamino_generate: NULL argument");
+    if (l->generated) return fail(UFOB_ERR_INVALID, "lamino-backproject: the volume was already generated");
+    if (l->pushed != l->num_projections)
+        return fail(UFOB_ERR_INVALID, "lamino-backproject received %u projections out of %u", l->pushed,
+                    l->num_projections);
+    UFOB_TRY(lamino_compute(l, l->d_proj.as<float>(), l->pw, l->ph, d_vol, (cudaStream_t)stream));
+    l->generated = true;
+    return UFOB_OK;
+}
+
+extern "C" void ufob_lamino_destroy(ufob_lamino *l) { delete l; }

@@ -15,7 +15,8 @@ import math
 import os
 
 __all__ = ["lib", "UfobError", "get_task", "FilterTask", "BackprojectTask", "FBP", "GeneralBackprojectTask",
-           "Batch", "FlatFieldCorrectTask", "ConeBeamProjectionWeightTask", "TransposeProjectionsTask", "StackedBackprojectTask", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
+           "Batch", "FlatFieldCorrectTask", "ConeBeamProjectionWeightTask", "TransposeProjectionsTask", "StackedBackprojectTask",
+           "LaminoBackprojectTask", "F32", "F16", "BF16", "F64", "U8", "U16", "U32", "ROWS", "PAIRS", "QUADS"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libufob.so")
@@ -144,6 +145,16 @@ def lib():
             "ufob_stacked_bp_get_requisition": ([vp, u32, u32, pu32, pu32], i),
             "ufob_stacked_bp_run": ([vp, vp, u32, u32, u32, vp, vp], i),
             "ufob_stacked_bp_destroy": ([vp], None),
+            "ufob_lamino_create": ([ctypes.POINTER(vp)], i),
+            "ufob_lamino_set_property": ([vp, cs, d], i),
+            "ufob_lamino_set_property_string": ([vp, cs, cs], i),
+            "ufob_lamino_set_array": ([vp, cs, vp, u32], i),
+            "ufob_lamino_setup": ([vp], i),
+            "ufob_lamino_get_requisition": ([vp, pu32, pu32, pu32], i),
+            "ufob_lamino_run": ([vp, vp, u32, u32, vp, vp], i),
+            "ufob_lamino_process": ([vp, vp, u32, u32, vp], i),
+            "ufob_lamino_generate": ([vp, vp, vp], i),
+            "ufob_lamino_destroy": ([vp], None),
             "ufob_ffc_props_init": ([ctypes.POINTER(FFCProps)], None),
             "ufob_ffc_set_property": ([ctypes.POINTER(FFCProps), cs, d], i),
             "ufob_flat_field_correct": ([ctypes.POINTER(FFCProps), vp, vp, vp, u32, u32, u32, vp, vp], i),
@@ -595,6 +606,67 @@ class StackedBackprojectTask(_Task):
         return out[0] if squeeze else out
 
 
+class LaminoBackprojectTask(_Task):
+    """``lamino-backproject`` (a reductor).  Array properties x-region, y-region
+    (integers from, to, step), region (the swept parameter's from, to, step),
+    projection-offset, center; numbers z, num-projections, overall-angle,
+    tomo-angle, lamino-angle, roll-angle; strings parameter ("z", "x-center",
+    "lamino-angle", "roll-angle") and addressing-mode."""
+
+    ARRAYS = ("x-region", "y-region", "region", "projection-offset", "center")
+
+    def __init__(self, **props):
+        super().__init__()
+        L = lib()
+        h = ctypes.c_void_p()
+        check(L.ufob_lamino_create(ctypes.byref(h)))
+        self._h = h
+        self._set_num, self._set_str, self._destroy = (L.ufob_lamino_set_property, L.ufob_lamino_set_property_string,
+                                                       L.ufob_lamino_destroy)
+        for k, v in props.items():
+            self.set_property(k.replace("_", "-"), v)
+
+    def set_property(self, name, value):
+        if name in self.ARRAYS:
+            import numpy as np
+            arr = np.ascontiguousarray(value, dtype=np.float64).reshape(-1)
+            check(lib().ufob_lamino_set_array(self._h, name.encode(), arr.ctypes.data, arr.size))
+            self._values[name] = tuple(arr)
+        else:
+            super().set_property(name, value)
+
+    def setup(self):
+        check(lib().ufob_lamino_setup(self._h))
+
+    def get_requisition(self):
+        x, y, z = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().ufob_lamino_get_requisition(self._h, ctypes.byref(x), ctypes.byref(y), ctypes.byref(z)))
+        return x.value, y.value, z.value
+
+    def process(self, proj, out=None, stream=None):
+        """All projections [n, H, W] (float32 CUDA) -> volume [nz, ny, nx]."""
+        import torch
+        proj = proj.contiguous()
+        _, H, W = proj.shape
+        self.setup()
+        nx, ny, nz = self.get_requisition()
+        out = torch.empty((nz, ny, nx), dtype=torch.float32, device=proj.device) if out is None else out
+        check(lib().ufob_lamino_run(self._h, _ptr(proj), W, H, _ptr(out), _stream(stream)))
+        return out
+
+    def push(self, projection, stream=None):
+        """The task's process(): one projection [H, W]."""
+        H, W = projection.shape
+        check(lib().ufob_lamino_process(self._h, _ptr(projection.contiguous()), W, H, _stream(stream)))
+
+    def generate(self, out=None, stream=None):
+        import torch
+        nx, ny, nz = self.get_requisition()
+        out = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda") if out is None else out
+        check(lib().ufob_lamino_generate(self._h, _ptr(out), _stream(stream)))
+        return out
+
+
 def _preprocess(ffc, dark, flat, cone):
     """ctypes Preprocess for the fused filter entry points (None when empty) and
     the objects it points into, to be kept alive over the call."""
@@ -744,7 +816,8 @@ def get_task(name, **props):
     """Create a task by its ufo-filters name."""
     table = {"filter": FilterTask, "backproject": BackprojectTask, "general-backproject": GeneralBackprojectTask,
              "flat-field-correct": FlatFieldCorrectTask, "cone-beam-projection-weight": ConeBeamProjectionWeightTask,
-             "transpose-projections": TransposeProjectionsTask, "stacked-backproject": StackedBackprojectTask}
+             "transpose-projections": TransposeProjectionsTask, "stacked-backproject": StackedBackprojectTask,
+             "lamino-backproject": LaminoBackprojectTask}
     if name not in table:
         raise KeyError("no task named %r (available: %s)" % (name, ", ".join(sorted(table))))
     return table[name](**props)

@@ -4,6 +4,7 @@
     python -m ufob.bench_configs --gbp      # only the general backprojection
     python -m ufob.bench_configs --pre      # only the preprocessing stages
     python -m ufob.bench_configs --stacked  # only stacked-backproject
+    python -m ufob.bench_configs --lamino   # only lamino-backproject
 
 * general backprojection: 1024 projections of 1024^2 over 360 degrees into a
   512^3 volume, for the cone geometry (source 800 px before the axis, detector
@@ -27,6 +28,10 @@
 
 * stacked-backproject (``--stacked``): 32 slices of 2048^2 from 1500 angles
   (uniform random sinograms) in the three precision modes.
+
+* lamino-backproject (``--lamino``): 1024 projections of 1024^2 into 512^3
+  at 30 degrees from the beam (the general-backproject lamino case through the
+  older task's surface).
 
 Units are voxel-angle updates per second (GUPS); times come from CUDA events
 after a warm-up call and average over repeated calls.
@@ -163,12 +168,29 @@ def bench_stacked(reps=2, Z=32, P=1500, W=2048, seed=11):
     return rows
 
 
+def bench_lamino(reps=2, n_proj=1024, det=1024, vol=512):
+    """lamino-backproject (30 degrees from the beam, the task's z parameter) of
+    1024 projections of 1024^2 into a 512^3 volume."""
+    import torch
+    from . import LaminoBackprojectTask
+    proj = torch.rand(n_proj, det, det, device="cuda")
+    h = vol // 2
+    t = LaminoBackprojectTask(num_projections=n_proj, x_region=(-h, h, 1), y_region=(-h, h, 1),
+                              region=(float(-h), float(h), 1.0), center=(det / 2.0, det / 2.0),
+                              lamino_angle=math.pi / 2 - math.pi / 6, overall_angle=2 * math.pi)
+    v = t.process(proj)
+    ms = _timeit(lambda: t.process(proj, out=v), reps)
+    return [{"workload": "lamino-backproject, %d projections of %d^2 -> %d^3" % (n_proj, det, vol),
+             "ms": round(ms, 2), "gups": round(float(vol) ** 3 * n_proj / ms / 1e6, 1)}]
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--gbp", action="store_true", help="only the general backprojection")
     ap.add_argument("--batch", action="store_true", help="only the uneven batch")
     ap.add_argument("--pre", action="store_true", help="only the preprocessing stages")
     ap.add_argument("--stacked", action="store_true", help="only stacked-backproject")
+    ap.add_argument("--lamino", action="store_true", help="only lamino-backproject")
     ap.add_argument("--projections", type=int, default=1024)
     ap.add_argument("--detector", type=int, default=1024)
     ap.add_argument("--volume", type=int, default=512)
@@ -176,7 +198,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
-    only = args.gbp or args.batch or args.pre or args.stacked
+    only = args.gbp or args.batch or args.pre or args.stacked or args.lamino
     if args.gbp or not only:
         rows += bench_gbp(args.reps, args.projections, args.detector, args.volume)
     if args.batch or not only:
@@ -185,6 +207,8 @@ def main(argv=None):
         rows += bench_pre()
     if args.stacked or not only:
         rows += bench_stacked()
+    if args.lamino or not only:
+        rows += bench_lamino()
     device_status()
     for r in rows:
         print(json.dumps(r))
