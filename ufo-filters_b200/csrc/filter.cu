@@ -27,6 +27,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "ufob_internal.h"
 
@@ -34,6 +35,17 @@ namespace ufob {
 
 static constexpr uint32_t kMaxFusedFFT = 8192;
 static constexpr int kFilterThreads = 256;
+
+// The register-radix kernel serves FFT widths 256..4096 unless UFOB_FILTER_RADIX4=1 selects the
+// shared-memory radix-4 kernel for every width (comparison and fallback).
+static bool fast_filter_enabled()
+{
+    static const int on = [] {
+        const char *e = getenv("UFOB_FILTER_RADIX4");
+        return (e && e[0] == '1') ? 0 : 1;
+    }();
+    return on != 0;
+}
 
 // ------------------------------------------------------------ host coefficient code
 
@@ -120,6 +132,35 @@ __global__ void k_twiddles(float2 *tw, uint32_t n)
     tw[m] = make_float2((float)c, (float)s);
 }
 
+// Per-pass twiddles of the register-radix kernel: [0, 64) pass 2, w^(2^b k) =
+// exp(-2 pi i 2^b k / 256) at b * 16 + k; then pass 3, exp(-2 pi i 2^b k / (256 R3))
+// at 64 + b * 256 + k for b < log2 R3 (R3 = n / 256).
+__global__ void k_pass_twiddles(float2 *tab, uint32_t n, uint32_t count)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    uint32_t b, k;
+    double den;
+    if (i < 64) {
+        b = i / 16;
+        k = i % 16;
+        den = 256.0;
+    } else {
+        b = (i - 64) / 256;
+        k = (i - 64) % 256;
+        den = (double)n;
+    }
+    double s, c;
+    sincospi(-2.0 * (double)(k << b) / den, &s, &c);
+    tab[i] = make_float2((float)c, (float)s);
+}
+
+static uint32_t pass_twiddle_count(uint32_t n)
+{
+    const uint32_t r3 = n / 256;
+    return 64 + 256 * (r3 >= 16 ? 4 : r3 >= 8 ? 3 : r3 >= 4 ? 2 : r3 >= 2 ? 1 : 0);
+}
+
 // In-place forward DFT of the interleaved pairs (ramp-fromreal, src/ufo-filter-task.c:317-334),
 // FP64, direct summation over an exact index m = j*k mod n.
 __global__ void k_dft_pairs_fp64(const float *in, float *out, uint32_t n)
@@ -180,6 +221,13 @@ ufob_status filter_plan_build(const ufob_filter_props &p, uint32_t nfft, FilterP
     k_twiddles<<<(nfft + T - 1) / T, T, 0, stream>>>(plan.d_twiddle.as<float2>(), nfft);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
+    if (nfft >= 256 && nfft <= 4096) {
+        const uint32_t cnt = pass_twiddle_count(nfft);
+        UFOB_TRY(plan.d_pass_tw.ensure(sizeof(float2) * cnt));
+        k_pass_twiddles<<<(cnt + T - 1) / T, T, 0, stream>>>(plan.d_pass_tw.as<float2>(), nfft, cnt);
+        UFOB_CUDA_TRY(cudaGetLastError());
+        note_launch();
+    }
     UFOB_CUDA_TRY(cudaStreamSynchronize(stream));
     plan.coeff.swap(c);
     plan.nfft = nfft;
@@ -283,41 +331,93 @@ __device__ __forceinline__ uint32_t pack_pair(float lo, float hi)
     }
 }
 
-// Filter two rows (one complex FFT of a + i b) in shared memory: rows 2*pair
-// and 2*pair+1, or for the slice-quad layout (OUT_F16_QUADS, `P` angles per
-// slice) item pair = (group * P + angle) * 2 + half, i.e. slices
-// 4*group + 2*half and 4*group + 2*half + 1 at one angle.
+// Rows of one work item (one complex FFT of a + i b): rows 2*pair and
+// 2*pair+1, or for the slice-quad layout (OUT_F16_QUADS, `P` angles per slice)
+// item pair = (group * P + angle) * 2 + half, i.e. slices 4*group + 2*half and
+// 4*group + 2*half + 1 at one angle.
+struct PairMap {
+    uint32_t ra, rb, half;
+    bool hasa, hasb;
+    size_t cell0;
+};
+
+template <int OUT>
+__device__ __forceinline__ PairMap map_pair(uint32_t pair, uint32_t rows, uint32_t P, uint32_t out_pitch)
+{
+    PairMap m;
+    m.ra = 2 * pair;
+    m.rb = 2 * pair + 1;
+    m.half = 0;
+    m.cell0 = 0;
+    m.hasa = m.ra < rows;
+    if (OUT == OUT_F16_QUADS) {
+        const uint32_t gp = pair >> 1;  // group * P + angle
+        m.half = pair & 1u;
+        const uint32_t grp = gp / P, ang = gp - grp * P;
+        m.ra = (4 * grp + 2 * m.half) * P + ang;
+        m.rb = m.ra + P;
+        m.hasa = m.ra < rows;
+        m.cell0 = (size_t)gp * out_pitch;
+    }
+    m.hasb = m.rb < rows;
+    return m;
+}
+
+// Store the filtered pair (X(n) = complex sample n: real = row a, imag = row b)
+// in the output layout; threads t0, t0 + step, ... share the row.
+template <int OUT, typename GET>
+__device__ __forceinline__ void store_pair(const PairMap &m, GET X, void *__restrict__ out, uint32_t out_w,
+                                           uint32_t out_pitch, uint32_t t0, uint32_t step)
+{
+    if (OUT == OUT_F16_QUADS) {
+        // words `half` (taps j-1) and 2 + `half` (taps j) of cell j; rows a, b in the low, high halves
+        uint32_t *o = reinterpret_cast<uint32_t *>(out) + m.cell0 * 4;
+        for (uint32_t j = t0; j < out_pitch; j += step) {
+            float2 lo = (j >= 1 && j - 1 < out_w) ? X(j - 1) : make_float2(0.f, 0.f);
+            float2 hi = (j < out_w) ? X(j) : make_float2(0.f, 0.f);
+            if (!m.hasa) lo.x = hi.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
+            if (!m.hasb) lo.y = hi.y = 0.f;
+            o[(size_t)j * 4 + m.half] = pack_pair<OUT>(lo.x, lo.y);
+            o[(size_t)j * 4 + 2 + m.half] = pack_pair<OUT>(hi.x, hi.y);
+        }
+    } else if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
+        uint32_t *o = reinterpret_cast<uint32_t *>(out);
+        for (uint32_t j = t0; j < out_pitch; j += step) {
+            float2 lo = (j >= 1 && j - 1 < out_w) ? X(j - 1) : make_float2(0.f, 0.f);
+            float2 hi = (j < out_w) ? X(j) : make_float2(0.f, 0.f);
+            o[(size_t)m.ra * out_pitch + j] = pack_pair<OUT>(lo.x, hi.x);
+            if (m.hasb) o[(size_t)m.rb * out_pitch + j] = pack_pair<OUT>(lo.y, hi.y);
+        }
+    } else {
+        for (uint32_t n = t0; n < out_w; n += step) {
+            float2 v = X(n);
+            store_value<OUT>(out, (size_t)m.ra * out_pitch + n, v.x);
+            if (m.hasb) store_value<OUT>(out, (size_t)m.rb * out_pitch + n, v.y);
+        }
+    }
+}
+
+// Filter one work item in shared memory with the radix-4 Stockham transform
+// (any power-of-two N up to 8192).
 template <int OUT, bool PRE>
 __device__ __forceinline__ void filter_pair(const RowSource &src, uint32_t width, uint32_t rows, uint32_t pair,
                                             float2 *bufA, float2 *bufB, const float2 *tw, const float2 *gains,
                                             uint32_t N, int log2N, void *__restrict__ out, uint32_t out_w,
                                             uint32_t out_pitch, uint32_t P = 0)
 {
-    uint32_t ra = 2 * pair, rb = 2 * pair + 1, half = 0;
-    size_t cell0 = 0;
-    bool hasa = true;
-    if (OUT == OUT_F16_QUADS) {
-        const uint32_t gp = pair >> 1;  // group * P + angle
-        half = pair & 1u;
-        const uint32_t grp = gp / P, ang = gp - grp * P;
-        ra = (4 * grp + 2 * half) * P + ang;
-        rb = ra + P;
-        hasa = ra < rows;
-        cell0 = (size_t)gp * out_pitch;
-    }
-    const bool hasb = rb < rows;
+    const PairMap m = map_pair<OUT>(pair, rows, P, out_pitch);
     uint32_t ya, pa_proj, yb, pb_proj;
-    const float *pa = row_start(src, hasa ? ra : 0, ya, pa_proj);
-    const float *pb = row_start(src, hasb ? rb : 0, yb, pb_proj);
+    const float *pa = row_start(src, m.hasa ? m.ra : 0, ya, pa_proj);
+    const float *pb = row_start(src, m.hasb ? m.rb : 0, yb, pb_proj);
     __syncthreads();  // previous pair's output reads of bufA/bufB (and table loads) are done
     for (uint32_t n = threadIdx.x; n < N; n += blockDim.x) {
         float a = 0.f, b = 0.f;
         if (n < width) {  // zero padding to N comes after the preprocessing
-            if (hasa) a = __ldg(pa + n);
-            if (hasb) b = __ldg(pb + n);
+            if (m.hasa) a = __ldg(pa + n);
+            if (m.hasb) b = __ldg(pb + n);
             if (PRE) {
-                if (hasa) a = preprocess_value(src, a, n, ya, pa_proj);
-                if (hasb) b = preprocess_value(src, b, n, yb, pb_proj);
+                if (m.hasa) a = preprocess_value(src, a, n, ya, pa_proj);
+                if (m.hasb) b = preprocess_value(src, b, n, yb, pb_proj);
             }
         }
         bufA[n] = make_float2(a, b);
@@ -326,43 +426,18 @@ __device__ __forceinline__ void filter_pair(const RowSource &src, uint32_t width
     float2 *Z = fft_smem<false>(bufA, bufB, tw, N, log2N);
     // separate, filter, recombine (pairs (k, N-k) are disjoint across threads)
     for (uint32_t k = threadIdx.x; k <= N / 2; k += blockDim.x) {
-        const uint32_t m = (N - k) & (N - 1);
-        float2 zk = Z[k], zm = Z[m], g = gains[k];
+        const uint32_t mm = (N - k) & (N - 1);
+        float2 zk = Z[k], zm = Z[mm], g = gains[k];
         float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
         float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
         ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
         Z[k] = make_float2(ax - by, ay + bx);
-        if (m != k) Z[m] = make_float2(ax + by, bx - ay);
+        if (mm != k) Z[mm] = make_float2(ax + by, bx - ay);
     }
     __syncthreads();
     float2 *other = (Z == bufA) ? bufB : bufA;
     float2 *X = fft_smem<true>(Z, other, tw, N, log2N);
-    if (OUT == OUT_F16_QUADS) {
-        // words `half` (taps j-1) and 2 + `half` (taps j) of cell j; rows a, b in the low, high halves
-        uint32_t *o = reinterpret_cast<uint32_t *>(out) + cell0 * 4;
-        for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
-            float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
-            float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
-            if (!hasa) lo.x = hi.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
-            if (!hasb) lo.y = hi.y = 0.f;
-            o[(size_t)j * 4 + half] = pack_pair<OUT>(lo.x, lo.y);
-            o[(size_t)j * 4 + 2 + half] = pack_pair<OUT>(hi.x, hi.y);
-        }
-    } else if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
-        uint32_t *o = reinterpret_cast<uint32_t *>(out);
-        for (uint32_t j = threadIdx.x; j < out_pitch; j += blockDim.x) {
-            float2 lo = (j >= 1 && j - 1 < out_w) ? X[j - 1] : make_float2(0.f, 0.f);
-            float2 hi = (j < out_w) ? X[j] : make_float2(0.f, 0.f);
-            o[(size_t)ra * out_pitch + j] = pack_pair<OUT>(lo.x, hi.x);
-            if (hasb) o[(size_t)rb * out_pitch + j] = pack_pair<OUT>(lo.y, hi.y);
-        }
-    } else {
-        for (uint32_t n = threadIdx.x; n < out_w; n += blockDim.x) {
-            float2 v = X[n];
-            store_value<OUT>(out, (size_t)ra * out_pitch + n, v.x);
-            if (hasb) store_value<OUT>(out, (size_t)rb * out_pitch + n, v.y);
-        }
-    }
+    store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, threadIdx.x, blockDim.x);
 }
 
 template <int OUT, bool PRE>
@@ -383,6 +458,274 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_rows(const RowSource 
 
     for (uint32_t pair = blockIdx.x; pair < npairs; pair += gridDim.x)
         filter_pair<OUT, PRE>(src, width, rows, pair, bufA, bufB, tw, gains, N, log2N, out, out_w, out_pitch, P);
+}
+
+// ------------------------------------------------------------ register-radix kernel (N = 256 .. 4096)
+//
+// A team of T = N / 16 threads transforms one work item; every thread holds 16
+// complex values in registers and each Stockham pass is a radix-16 (or, for the
+// last pass, radix N / 256) DFT in registers followed by one exchange through
+// shared memory: 2 or 3 passes per transform instead of log4 N radix-4 passes,
+// 7 barriers per work item.  Shared indices are XOR-swizzled, i ^ ((i >> 4) &
+// 15), which makes the stride-16 stores of the first pass conflict-free.
+// Twiddles of pass p come from a per-pass table w^(2^b * k), b < log2 radix,
+// and the others are products of at most three of them.  Two or more teams
+// share a 256-thread CTA and move in lock step.
+
+static constexpr int kFastThreads = 256;
+
+__device__ __forceinline__ uint32_t swz(uint32_t i) { return i ^ ((i >> 4) & 15u); }
+
+template <bool INV>
+__device__ __forceinline__ float2 mul_mi(float2 a)  // a * (-i) forward, a * (+i) inverse
+{
+    return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// a * (c, s) with s negated for the inverse transform
+template <bool INV>
+__device__ __forceinline__ float2 mulc(float2 a, float c, float s)
+{
+    if (INV) s = -s;
+    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &x0, float2 &x1, float2 &x2, float2 &x3)
+{
+    const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<INV>(csub(x1, x3));
+    x0 = cadd(t0, t2);
+    x2 = csub(t0, t2);
+    x1 = cadd(t1, t3);
+    x3 = csub(t1, t3);
+}
+
+// In-place DFT of R points in natural order (R = 2, 4, 8, 16), forward e^{-2 pi i nk/R}.
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 *v)
+{
+    constexpr float r2 = 0.70710678118654752440f;
+    constexpr float c1 = 0.92387953251128675613f;  // cos(pi/8)
+    constexpr float s1 = 0.38268343236508977173f;  // sin(pi/8)
+    if (R == 2) {
+        const float2 a = v[0];
+        v[0] = cadd(a, v[1]);
+        v[1] = csub(a, v[1]);
+    } else if (R == 4) {
+        dft4<INV>(v[0], v[1], v[2], v[3]);
+    } else if (R == 8) {
+        // x[n1 + 2 n2]: DFT4 over n2, twiddle W8^(n1 k2), DFT2 over n1 -> X[k2 + 4 k1]
+        dft4<INV>(v[0], v[2], v[4], v[6]);
+        dft4<INV>(v[1], v[3], v[5], v[7]);
+        v[3] = mulc<INV>(v[3], r2, -r2);
+        v[5] = mul_mi<INV>(v[5]);
+        v[7] = mulc<INV>(v[7], -r2, -r2);
+        float2 o[8];
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) {
+            o[k2] = cadd(v[2 * k2], v[2 * k2 + 1]);
+            o[k2 + 4] = csub(v[2 * k2], v[2 * k2 + 1]);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = o[i];
+    } else {
+        // x[n1 + 4 n2]: DFT4 over n2, twiddle W16^(n1 k2), DFT4 over n1 -> X[k2 + 4 k1]
+#pragma unroll
+        for (int n1 = 0; n1 < 4; n1++) dft4<INV>(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+        // y[n1][k2] sits in v[n1 + 4 k2]
+        v[1 + 4] = mulc<INV>(v[1 + 4], c1, -s1);    // W^1
+        v[1 + 8] = mulc<INV>(v[1 + 8], r2, -r2);    // W^2
+        v[1 + 12] = mulc<INV>(v[1 + 12], s1, -c1);  // W^3
+        v[2 + 4] = mulc<INV>(v[2 + 4], r2, -r2);    // W^2
+        v[2 + 8] = mul_mi<INV>(v[2 + 8]);           // W^4
+        v[2 + 12] = mulc<INV>(v[2 + 12], -r2, -r2); // W^6
+        v[3 + 4] = mulc<INV>(v[3 + 4], s1, -c1);    // W^3
+        v[3 + 8] = mulc<INV>(v[3 + 8], -r2, -r2);   // W^6
+        v[3 + 12] = mulc<INV>(v[3 + 12], -c1, s1);  // W^9
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) dft4<INV>(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3]);
+        // X[k2 + 4 k1] sits in v[k1 + 4 k2]: transpose the 4x4 block
+        float2 o[16];
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++)
+#pragma unroll
+            for (int k1 = 0; k1 < 4; k1++) o[k2 + 4 * k1] = v[k1 + 4 * k2];
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = o[i];
+    }
+}
+
+// v[m] *= w^(m k) for m < R, with w^(2^b k) = tab[b * Ns + k]
+template <int R, bool INV>
+__device__ __forceinline__ void twiddle(float2 *v, const float2 *tab, uint32_t k, uint32_t Ns)
+{
+    float2 w[R];
+    w[1] = tab[k];
+    if (R >= 4) w[2] = tab[Ns + k];
+    if (R >= 8) w[4] = tab[2 * Ns + k];
+    if (R >= 16) w[8] = tab[3 * Ns + k];
+    if (INV) {
+        w[1].y = -w[1].y;
+        if (R >= 4) w[2].y = -w[2].y;
+        if (R >= 8) w[4].y = -w[4].y;
+        if (R >= 16) w[8].y = -w[8].y;
+    }
+    if (R >= 4) w[3] = cmul(w[1], w[2]);
+    if (R >= 8) {
+        w[5] = cmul(w[1], w[4]);
+        w[6] = cmul(w[2], w[4]);
+        w[7] = cmul(w[3], w[4]);
+    }
+    if (R >= 16) {
+#pragma unroll
+        for (int m = 9; m < 16; m++) w[m] = cmul(w[m - 8], w[8]);
+    }
+#pragma unroll
+    for (int m = 1; m < R; m++) v[m] = cmul(v[m], w[m]);
+}
+
+// One Stockham pass (Ns > 1) of radix R over N points, shared src -> shared dst;
+// thread t of a team of T handles butterflies t, t + T, ... (16 / R of them).
+template <int R, bool INV>
+__device__ __forceinline__ void fast_pass(const float2 *src, float2 *dst, const float2 *tab, uint32_t N, uint32_t Ns,
+                                          uint32_t t, uint32_t T)
+{
+#pragma unroll
+    for (int q = 0; q < 16 / R; q++) {
+        const uint32_t j = t + q * T;
+        const uint32_t k = j & (Ns - 1);
+        float2 v[R];
+#pragma unroll
+        for (int m = 0; m < R; m++) v[m] = src[swz(j + m * (N / R))];
+        twiddle<R, INV>(v, tab, k, Ns);
+        dft<R, INV>(v);
+        const uint32_t base = (j - k) * R + k;
+#pragma unroll
+        for (int m = 0; m < R; m++) dst[swz(base + m * Ns)] = v[m];
+    }
+}
+
+// Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer.
+template <int LOGN, bool INV>
+__device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 *tab2, const float2 *tab3,
+                                             uint32_t t, uint32_t T)
+{
+    constexpr uint32_t N = 1u << LOGN;
+    constexpr int R3 = (int)(N / 256);
+    fast_pass<16, INV>(a, b, tab2, N, 16, t, T);
+    __syncthreads();
+    if (R3 == 1) return b;
+    fast_pass<(R3 > 1 ? R3 : 2), INV>(b, a, tab3, N, 256, t, T);
+    __syncthreads();
+    return a;
+}
+
+template <int OUT, bool PRE, int LOGN>
+__global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource src, uint32_t width, uint32_t rows,
+                                                             const float2 *__restrict__ g_tab,
+                                                             const float2 *__restrict__ g_gains,
+                                                             void *__restrict__ out, uint32_t out_w,
+                                                             uint32_t out_pitch, uint32_t npairs, uint32_t P)
+{
+    constexpr uint32_t N = 1u << LOGN, T = N / 16, TEAMS = kFastThreads / T;
+    constexpr uint32_t R3 = N / 256, LR3 = R3 >= 16 ? 4 : R3 >= 8 ? 3 : R3 >= 4 ? 2 : R3 >= 2 ? 1 : 0;
+    constexpr uint32_t NTAB = 4 * 16 + LR3 * 256;
+    extern __shared__ float4 smem_f4[];
+    float2 *sm = reinterpret_cast<float2 *>(smem_f4);
+    float2 *tab2 = sm, *tab3 = sm + 64, *gains = sm + NTAB;
+    const uint32_t team = threadIdx.x / T, t = threadIdx.x - team * T;
+    float2 *bufA = gains + (N / 2 + 2) + team * 2 * N, *bufB = bufA + N;
+    for (uint32_t i = threadIdx.x; i < NTAB; i += kFastThreads) sm[i] = g_tab[i];
+    for (uint32_t i = threadIdx.x; i <= N / 2; i += kFastThreads) gains[i] = g_gains[i];
+
+    const uint32_t iters = (npairs + gridDim.x * TEAMS - 1) / (gridDim.x * TEAMS);
+    for (uint32_t it = 0; it < iters; it++) {
+        const uint32_t pair = (it * gridDim.x + blockIdx.x) * TEAMS + team;
+        const bool live = pair < npairs;
+        const PairMap m = map_pair<OUT>(live ? pair : 0, live ? rows : 0, P, out_pitch);
+        // pass 1 loads straight from global memory: elements t + m N/16 of rows a, b
+        float2 v[16];
+        {
+            uint32_t ya, pa_, yb, pb_;
+            const float *ra = row_start(src, m.hasa ? m.ra : 0, ya, pa_);
+            const float *rb = row_start(src, m.hasb ? m.rb : 0, yb, pb_);
+            if (!PRE) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const uint32_t n = t + q * T;
+                    float a = 0.f, b = 0.f;
+                    if (n < width) {
+                        if (m.hasa) a = __ldg(ra + n);
+                        if (m.hasb) b = __ldg(rb + n);
+                    }
+                    v[q] = make_float2(a, b);
+                }
+            } else {
+                // every load of a half (data, dark, flat) is issued before the dependent divisions
+                // and logarithms; rows past the stack read row 0 and are zeroed afterwards
+                const float *da = src.dark ? src.dark + (size_t)ya * src.corr_pitch : nullptr;
+                const float *fa = src.dark ? src.flat + (size_t)ya * src.corr_pitch : nullptr;
+                const float *db = src.dark ? src.dark + (size_t)yb * src.corr_pitch : nullptr;
+                const float *fb = src.dark ? src.flat + (size_t)yb * src.corr_pitch : nullptr;
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    float xa[8], xb[8], dka[8], fla[8], dkb[8], flb[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const uint32_t n = t + (8 * h + i) * T;
+                        const uint32_t nn = n < width ? n : 0;
+                        xa[i] = __ldg(ra + nn);
+                        xb[i] = __ldg(rb + nn);
+                        if (src.dark) {
+                            dka[i] = __ldg(da + nn);
+                            fla[i] = __ldg(fa + nn);
+                            dkb[i] = __ldg(db + nn);
+                            flb[i] = __ldg(fb + nn);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        const uint32_t n = t + (8 * h + i) * T;
+                        float a = xa[i], b = xb[i];
+                        if (src.dark) {
+                            a = ffc_value(src, a, dka[i], fla[i]);
+                            b = ffc_value(src, b, dkb[i], flb[i]);
+                        }
+                        if (src.cone) {
+                            a = preprocess_value(src.cone_only(), a, n, ya, pa_);
+                            b = preprocess_value(src.cone_only(), b, n, yb, pb_);
+                        }
+                        const bool in = n < width;
+                        v[8 * h + i] = make_float2(in && m.hasa ? a : 0.f, in && m.hasb ? b : 0.f);
+                    }
+                }
+            }
+        }
+        __syncthreads();  // tables loaded; the previous item's output reads are done
+        dft<16, false>(v);
+#pragma unroll
+        for (int q = 0; q < 16; q++) bufA[swz(t * 16 + q)] = v[q];
+        __syncthreads();
+        const float2 *Z = fast_tail<LOGN, false>(bufA, bufB, tab2, tab3, t, T);
+        float2 *O = (Z == bufA) ? bufB : bufA;
+        // separate the two rows' spectra, apply the gains, recombine (element e = t + q N/16)
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            const uint32_t e = t + q * T;
+            const uint32_t k = e <= N / 2 ? e : N - e;
+            const float2 zk = Z[swz(k)], zm = Z[swz((N - k) & (N - 1))], g = gains[k];
+            float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
+            float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
+            ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
+            v[q] = e <= N / 2 ? make_float2(ax - by, ay + bx) : make_float2(ax + by, bx - ay);
+        }
+        dft<16, true>(v);
+#pragma unroll
+        for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
+        __syncthreads();
+        const float2 *X = fast_tail<LOGN, true>(O, O == bufA ? bufB : bufA, tab2, tab3, t, T);
+        if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[swz(i)]; }, out, out_w, out_pitch, t, T);
+    }
 }
 
 // Persistent filter stage of an uneven batch: work items (job, row pair) are
@@ -447,12 +790,53 @@ static ufob_status launch_rows_t(const FilterPlan &plan, const RowSource &src, u
     return UFOB_OK;
 }
 
+template <int OUT, bool PRE, int LOGN>
+static ufob_status launch_fast_t(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                                 void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P)
+{
+    constexpr uint32_t N = 1u << LOGN, TEAMS = kFastThreads / (N / 16);
+    const size_t smem = sizeof(float2) * (pass_twiddle_count(N) + N / 2 + 2 + (size_t)TEAMS * 2 * N);
+    auto kern = k_filter_fast<OUT, PRE, LOGN>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, smem));
+    if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);
+    const uint32_t npairs = OUT == OUT_F16_QUADS ? (rows / P + 3) / 4 * P * 2 : (rows + 1) / 2;
+    uint32_t grid = (uint32_t)num_sms() * (uint32_t)per_sm;
+    grid = std::min(grid, (npairs + TEAMS - 1) / TEAMS);
+    if (grid == 0) return UFOB_OK;
+    kern<<<grid, kFastThreads, smem, s>>>(src, width, rows, plan.d_pass_tw.as<float2>(), plan.d_gains.as<float2>(),
+                                          d_out, out_w, out_pitch, npairs, P);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+template <int OUT, bool PRE>
+static ufob_status launch_rows_p(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
+                                 void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P)
+{
+    if (fast_filter_enabled()) switch (plan.nfft) {
+        case 256: return launch_fast_t<OUT, PRE, 8>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+        case 512: return launch_fast_t<OUT, PRE, 9>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+        case 1024: return launch_fast_t<OUT, PRE, 10>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+        case 2048: return launch_fast_t<OUT, PRE, 11>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+        case 4096: return launch_fast_t<OUT, PRE, 12>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+        default: break;
+        }
+    return launch_rows_t<OUT, PRE>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+}
+
 template <int OUT>
 static ufob_status launch_rows(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
                                void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P = 0)
 {
-    if (src.has_pre()) return launch_rows_t<OUT, true>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
-    return launch_rows_t<OUT, false>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+    if (src.has_pre()) return launch_rows_p<OUT, true>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
+    return launch_rows_p<OUT, false>(plan, src, width, rows, d_out, out_w, out_pitch, s, P);
 }
 
 ufob_status filter_rows_launch_src(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,

@@ -69,6 +69,7 @@ struct FilterPlan {
     DevBuf d_coeff;            // same on the device (float)
     DevBuf d_gains;            // float2 [nfft/2 + 1]: symmetrised per-bin gains
     DevBuf d_twiddle;          // float2 [nfft]: exp(-2 pi i m / nfft), FP64-computed
+    DevBuf d_pass_tw;          // float2: per-pass twiddles of the register-radix kernel (256 <= nfft <= 4096)
 };
 
 // Host restatement of the reference's coefficient builders (before the
@@ -113,6 +114,15 @@ struct RowSource {
     int absorption = 0, fix_abnormal = 0;
     const ConeParams *cone = nullptr;
     bool has_pre() const { return dark != nullptr || cone != nullptr; }
+#ifdef __CUDACC__
+    __host__ __device__
+#endif
+    RowSource cone_only() const  // the same source without its flat-field step
+    {
+        RowSource r = *this;
+        r.dark = r.flat = nullptr;
+        return r;
+    }
 };
 
 #ifdef __CUDACC__
@@ -134,15 +144,22 @@ UFOB_HD inline RowSource plain_rows(const float *base, uint32_t pitch)
 // Detector row `y` (relative to the dark/flat base) and projection `p` of one
 // row; x = detector column.  FP32 with the reference's operation order, IEEE
 // division and square root.
+// Flat-field correction of value v with its dark and flat values (ffc.cl:31-45).
+__device__ __forceinline__ float ffc_value(const RowSource &s, float v, float dark, float flat)
+{
+    const float cd = __fmul_rn(dark, s.dark_scale);
+    const float cf = __fmul_rn(flat, s.flat_scale);
+    v = s.absorption ? logf(__fdiv_rn(__fsub_rn(cf, cd), __fsub_rn(v, cd)))
+                     : __fdiv_rn(__fsub_rn(v, cd), __fsub_rn(cf, cd));
+    if (s.fix_abnormal && !isfinite(v)) v = 0.f;
+    return v;
+}
+
 __device__ __forceinline__ float preprocess_value(const RowSource &s, float v, uint32_t x, uint32_t y, uint32_t p)
 {
-    if (s.dark) {  // ffc.cl:31-45
+    if (s.dark) {
         const size_t i = (size_t)y * s.corr_pitch + x;
-        const float cd = __fmul_rn(__ldg(s.dark + i), s.dark_scale);
-        const float cf = __fmul_rn(__ldg(s.flat + i), s.flat_scale);
-        v = s.absorption ? logf(__fdiv_rn(__fsub_rn(cf, cd), __fsub_rn(v, cd)))
-                         : __fdiv_rn(__fsub_rn(v, cd), __fsub_rn(cf, cd));
-        if (s.fix_abnormal && !isfinite(v)) v = 0.f;
+        v = ffc_value(s, v, __ldg(s.dark + i), __ldg(s.flat + i));
     }
     if (s.cone) {  // conebeam.cl:29-35
         const ConeParams c = s.cone[p];
