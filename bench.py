@@ -389,7 +389,8 @@ def main():
         pass
     f_ms, f_n = chosen["kernel_ms_per_step"]["filter"], chosen["kernel_launches_per_step"]["filter"]
     f_bytes = Z * P * W * 4.0 + Z * P * (W if storage == ufob.F32 else (W + 1)) * 4.0
-    roofline_filter = {"bound": "hbm", "kernel": "k_filter_rows", "achieved": f_bytes / (f_ms * 1e-3) / 1e9,
+    f_kernel = "k_filter_fast" if 256 <= W <= 4096 and os.environ.get("UFOB_FILTER_RADIX4") != "1" else "k_filter_rows"
+    roofline_filter = {"bound": "hbm", "kernel": f_kernel, "achieved": f_bytes / (f_ms * 1e-3) / 1e9,
                        "peak": hbm_peak, "unit": "GB/s",
                        "frac": (f_bytes / (f_ms * 1e-3) / 1e9) / hbm_peak if hbm_peak else None,
                        "peak_source": "MEASURED_PEAKS.json hbm_gbs"}
