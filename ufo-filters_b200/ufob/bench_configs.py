@@ -191,6 +191,7 @@ def main(argv=None):
     ap.add_argument("--pre", action="store_true", help="only the preprocessing stages")
     ap.add_argument("--stacked", action="store_true", help="only stacked-backproject")
     ap.add_argument("--lamino", action="store_true", help="only lamino-backproject")
+    ap.add_argument("--pre-rows", type=int, default=256, help="detector rows of the preprocessing workload")
     ap.add_argument("--projections", type=int, default=1024)
     ap.add_argument("--detector", type=int, default=1024)
     ap.add_argument("--volume", type=int, default=512)
@@ -204,7 +205,7 @@ def main(argv=None):
     if args.batch or not only:
         rows += bench_batch()
     if args.pre or not only:
-        rows += bench_pre()
+        rows += bench_pre(rows=args.pre_rows)
     if args.stacked or not only:
         rows += bench_stacked()
     if args.lamino or not only:
