@@ -1,6 +1,7 @@
 """Train and evaluate the 90-angle sparse-view correction network.
 
     python -m ufob.train_cnn --pairs 20000 --epochs 8 --ckpt cnn.npz
+    python -m ufob.train_cnn --pretrained          # evaluate and time the shipped weights
 
 Pairs (90-angle FBP, 1800-angle FBP) of seeded random-ellipse phantoms at
 512^2 are made on the GPU by the engine's own projector and FBP and cached in
@@ -80,16 +81,22 @@ def main(argv=None):
     ap.add_argument("--ckpt-every", type=int, default=1000)
     ap.add_argument("--log-every", type=int, default=250)
     ap.add_argument("--eval-only", action="store_true")
+    ap.add_argument("--pretrained", action="store_true", help="evaluate the shipped weights (implies --eval-only)")
+    ap.add_argument("--time-batches", default="64,128,256", help="batch sizes of the timing comparison")
     args = ap.parse_args(argv)
 
     import torch
     from .cnn import PairMaker, SparseViewNet, rel_l2
 
     maker = PairMaker()
-    net = SparseViewNet(seed=1234)
     start = 0
-    if args.ckpt and os.path.exists(args.ckpt):
-        start = int(net.load(args.ckpt).get("train_step", 0))
+    if args.pretrained:
+        net = SparseViewNet.pretrained()
+        args.eval_only = True
+    else:
+        net = SparseViewNet(seed=1234)
+        if args.ckpt and os.path.exists(args.ckpt):
+            start = int(net.load(args.ckpt).get("train_step", 0))
     steps = int(math.ceil(args.epochs * args.pairs / args.batch))
     report = {"pairs": args.pairs, "batch": args.batch, "steps": steps, "resumed_at": start}
     t0 = time.time()
@@ -127,7 +134,7 @@ def main(argv=None):
     report["eval"] = {"seeds": [args.eval_base, args.eval_base + args.eval_count],
                       "plain_fbp90_rel_l2": round(float(torch.cat(e_plain).mean()), 5),
                       "cnn_rel_l2": round(float(torch.cat(e_net).mean()), 5)}
-    report["time_per_slice"] = [time_paths(net, maker, B=b) for b in (64, 128)]
+    report["time_per_slice"] = [time_paths(net, maker, B=int(b)) for b in args.time_batches.split(",")]
     print(json.dumps(report))
 
 
