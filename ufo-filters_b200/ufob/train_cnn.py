@@ -65,6 +65,8 @@ def time_paths(net, maker, B=64, reps=5):
         out[name] = {"sparse_fbp_us": round(t_sparse, 2), "network_us": round(t_net, 2),
                      "learned_path_us": round(t_learned, 2), "dense_fbp_us": round(t_dense, 2),
                      "speedup_vs_dense": round(t_dense / t_learned, 2)}
+    # the engine's fastest learned path (FP16-storage sparse FBP + network) against the plain dense FBP
+    out["fp16_learned_vs_plain_dense"] = round(out["fp32"]["dense_fbp_us"] / out["fp16"]["learned_path_us"], 2)
     return out
 
 
@@ -125,15 +127,22 @@ def main(argv=None):
         del X, Y
         if args.ckpt:
             net.save(args.ckpt, train_step=steps)
-    e_plain, e_net = [], []
+    from . import F16, FBP
+    fbp16 = FBP(storage=F16)
+    e_plain, e_net, e_net16 = [], [], []
     eval_seeds = list(range(args.eval_base, args.eval_base + args.eval_count))
     for i in range(0, len(eval_seeds), 32):
-        x, y, _ = maker.pair(eval_seeds[i:i + 32])
+        imgs = maker.phantoms(eval_seeds[i:i + 32])
+        s_sparse = maker.sinograms(imgs, maker.sparse)
+        x = maker.fbp_sparse.process(s_sparse)
+        y = maker.fbp_dense.process(maker.sinograms(imgs, maker.dense))
         e_plain.append(rel_l2(x, y))
         e_net.append(rel_l2(net.forward(x), y))
+        e_net16.append(rel_l2(net.forward(fbp16.process(s_sparse)), y))
     report["eval"] = {"seeds": [args.eval_base, args.eval_base + args.eval_count],
                       "plain_fbp90_rel_l2": round(float(torch.cat(e_plain).mean()), 5),
-                      "cnn_rel_l2": round(float(torch.cat(e_net).mean()), 5)}
+                      "cnn_rel_l2": round(float(torch.cat(e_net).mean()), 5),
+                      "cnn_on_fp16_fbp90_rel_l2": round(float(torch.cat(e_net16).mean()), 5)}
     report["time_per_slice"] = [time_paths(net, maker, B=int(b)) for b in args.time_batches.split(",")]
     print(json.dumps(report))
 
