@@ -216,3 +216,61 @@ def test_fbp_from_raw_projections(cuda, storage, tol):
         np.testing.assert_array_equal(sub, got[2:7])
     else:  # the FP16 filter pairs slices (2g, 2g+1) in one complex FFT: other partners, other round-off
         assert oracle.rel_l2(sub, got[2:7]) < 1e-4
+
+
+def test_fused_sinogram_input_rows(cuda):
+    """sinogram-input: one dark/flat row for every row, applied in projection order."""
+    Z, P, W = 3, 50, 64
+    rng = np.random.default_rng(13)
+    dark = rng.uniform(90, 110, W).astype(np.float32)
+    flat = (dark + 1000).astype(np.float32)
+    data = (dark + rng.uniform(50, 1000, (Z, P, W))).astype(np.float32)
+    ffc = ufob.FlatFieldCorrectTask(sinogram_input=True, absorption_correct=True)
+    got = ufob.FilterTask().process_projections(_t(data), ffc=ffc, dark=_t(dark), flat=_t(flat),
+                                                sinograms=False).cpu().numpy()
+    ref = oracle.fft_filter_ifft(oracle.flat_field_correct(data, dark, flat, sinogram_input=True,
+                                                           absorption_correct=True))
+    assert got.shape == (Z, P, W)
+    assert oracle.rel_l2(got, ref) < 1e-5
+
+
+def test_fused_cone_weight_row_subrange(cuda):
+    """Detector rows first_row.. of each projection: the weight uses their absolute row."""
+    rng = np.random.default_rng(14)
+    N, H, W = 4, 16, 64
+    proj = rng.standard_normal((N, H, W)).astype(np.float32)
+    props = dict(center_position_x=30.0, center_position_z=7.5, source_distance=250.0, detector_distance=90.0,
+                 axis_angle_x=0.2)
+    cone = ufob.ConeBeamProjectionWeightTask(**props)
+    got = ufob.FilterTask().process_projections(_t(proj), cone=cone, sinograms=False, first_row=5,
+                                                n_rows=6).cpu().numpy()
+    ref = oracle.fft_filter_ifft(oracle.cone_beam_weight(proj, **props)[:, 5:11])
+    assert got.shape == (N, 6, W)
+    assert oracle.rel_l2(got, ref) < 1e-5
+
+
+@pytest.mark.parametrize("dtype,layout", [(ufob.F16, ufob.PAIRS), (ufob.BF16, ufob.PAIRS), (ufob.BF16, ufob.ROWS),
+                                          (ufob.F16, ufob.ROWS)])
+def test_fused_16bit_outputs_equal_unfused(cuda, dtype, layout):
+    N, H, W = 30, 5, 128
+    data, dark, flat = _frames(15, N, H, W)
+    ffc = ufob.FlatFieldCorrectTask(absorption_correct=1)
+    f = ufob.FilterTask()
+    got = f.process_projections(_t(data), ffc=ffc, dark=_t(dark), flat=_t(flat), dtype=dtype, layout=layout)
+    sinos = oracle.transpose_projections(ffc.process(_t(data), _t(dark), _t(flat)).cpu().numpy())
+    ref = f.process(_t(sinos), dtype=dtype, layout=layout)
+    assert got.shape == ref.shape
+    assert torch.equal(got, ref)
+
+
+def test_fused_rejections(cuda):
+    f = ufob.FilterTask()
+    data, dark, flat = _frames(16, 4, 3, 64)
+    ffc = ufob.FlatFieldCorrectTask()
+    with pytest.raises(ufob.UfobError):  # QUADS holds sinograms only
+        f.process_projections(_t(data), ffc=ffc, dark=_t(dark), flat=_t(flat), sinograms=False, dtype=ufob.F16,
+                              layout=ufob.QUADS)
+    with pytest.raises(ufob.UfobError):  # rows past the projection height
+        f.process_projections(_t(data), ffc=ffc, dark=_t(dark), flat=_t(flat), first_row=2, n_rows=2)
+    with pytest.raises(ValueError):
+        f.process_projections(_t(data), ffc=ffc)  # dark and flat missing
