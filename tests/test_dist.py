@@ -73,3 +73,50 @@ def test_single_process_context_is_a_no_op():
     ctx.barrier()
     start, stop, vol = udist.reconstruct_sharded(ctx, np.zeros((3, 4, 4)), lambda s: s + 1, gather=True)
     assert (start, stop) == (0, 3) and vol.shape == (3, 4, 4)
+
+
+CONE = {"source-position-y": -120.0, "detector-position-y": 40.0, "center-position-x": 16.0,
+        "center-position-z": 6.0}
+
+
+def _volume_worker(rank, world, port, proj, out_dir):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    ctx = udist.init(backend="gloo", timeout_s=60)
+    try:
+        n = proj.shape[0]
+        a, b = udist.slice_range(n, rank, world)
+        z0, z1, vol = udist.reconstruct_volume_sharded(
+            ctx, torch.from_numpy(proj[a:b]), n, (-4.0, 4.0, 1.0),
+            lambda p: oracle.fft_filter_ifft(np.asarray(p)).astype(np.float32),
+            lambda allp, reg: oracle.general_backproject(np.asarray(allp), n, region=reg, **CONE).astype(np.float32),
+            gather=True)
+        assert (z0, z1) == ((0, 8) if rank == 0 else udist.slice_range(8, rank, world))
+        if rank == 0:
+            np.save(os.path.join(out_dir, "vol.npy"), vol.numpy())
+        else:
+            assert vol is None
+    finally:
+        udist.finish(ctx)
+
+
+@pytest.mark.parametrize("n", [12, 13])
+def test_two_gloo_ranks_cone_volume_split_along_z(tmp_path, n):
+    """Each rank filters its share of the projections, one all-gather exchanges them, each rank
+    backprojects its z range; rank 0's gathered volume equals the one-process reconstruction."""
+    rng = np.random.default_rng(n)
+    proj = rng.standard_normal((n, 12, 32)).astype(np.float32)
+    mp.spawn(_volume_worker, args=(2, _free_port(), proj, str(tmp_path)), nprocs=2, join=True)
+    ref = oracle.general_backproject(oracle.fft_filter_ifft(proj).astype(np.float32), n, region=(-4.0, 4.0, 1.0),
+                                     **CONE).astype(np.float32)
+    np.testing.assert_array_equal(np.load(tmp_path / "vol.npy"), ref)
+
+
+def test_volume_sharded_single_process():
+    ctx = udist.Ctx()
+    proj = torch.zeros((3, 4, 8))
+    z0, z1, vol = udist.reconstruct_volume_sharded(ctx, proj, 3, (0.0, 5.0, 1.0), lambda p: p + 1,
+                                                   lambda allp, reg: torch.full((round((reg[1] - reg[0]) / reg[2] + 0.5), 2, 2), float(allp.sum())))
+    assert (z0, z1) == (0, 5) and vol.shape == (5, 2, 2) and float(vol[0, 0, 0]) == 96.0
+    with pytest.raises(ValueError):
+        udist.reconstruct_volume_sharded(ctx, proj[:2], 3, (0.0, 5.0, 1.0), lambda p: p, lambda a, r: a)

@@ -4,7 +4,13 @@ Parallel-beam slices are independent, so a stack is split into contiguous
 slice ranges, one per rank, and every rank reconstructs its own range with no
 collective in the data path.  The only collectives are the timing reductions
 (max over ranks) and, if the caller wants one volume on one host, a gather of
-the reconstructed slices to rank 0 at the end.  Rank/world come from the
+the reconstructed slices to rank 0 at the end.
+
+Cone-beam and laminography volumes (general-backproject) are partitioned
+along z instead: every slice needs every projection, so each rank filters its
+share of the projections, one all-gather gives every rank all filtered
+projections, and each rank backprojects its own z range
+(`reconstruct_volume_sharded`).  Rank/world come from the
 torchrun environment (RANK, WORLD_SIZE, LOCAL_RANK, MASTER_ADDR/PORT); the
 backend is NCCL when CUDA is available and gloo otherwise (CPU tests).
 """
@@ -100,3 +106,59 @@ def reconstruct_sharded(ctx, stack, reconstruct, gather=False):
         return 0, stack.shape[0], torch.cat(parts).cpu()
     ctx.group.send(t, dst=0)
     return start, stop, None
+
+
+def _all_gather_uneven(ctx, t, counts):
+    """All-gather of rank shares along dim 0 with counts[r] rows from rank r
+    (padded to the largest share for the collective); returns the concatenation."""
+    import torch
+    if ctx.group is None:
+        return t
+    mx = max(counts)
+    pad = t if t.shape[0] == mx else torch.cat([t, t.new_zeros((mx - t.shape[0],) + tuple(t.shape[1:]))])
+    parts = [torch.empty_like(pad) for _ in range(ctx.world)]
+    ctx.group.all_gather(parts, pad.contiguous())
+    return torch.cat([p[:c] for p, c in zip(parts, counts)])
+
+
+def reconstruct_volume_sharded(ctx, proj_share, n_projections, z_region, filter_fn, backproject_fn, gather=False):
+    """Filter this rank's share of the projections, exchange them, and backproject this
+    rank's z range.
+
+    proj_share: projections slice_range(n_projections, rank, world) of the stack
+    ([n_r, H, W], device tensor with NCCL, CPU tensor with gloo); z_region: the whole
+    volume's (from, to, step); filter_fn(projections) -> filtered projections;
+    backproject_fn(all_filtered, (from, to, step)) -> volume [nz_r, ny, nx] of this
+    rank's slices.  Returns (z0, z1, local volume); with `gather`, rank 0 receives the
+    whole volume (others get None)."""
+    import math
+    import torch
+    start, step = float(z_region[0]), float(z_region[2])
+    nz = int(math.ceil((float(z_region[1]) - start) / step))
+    counts = [b - a for a, b in (slice_range(n_projections, r, ctx.world) for r in range(ctx.world))]
+    if proj_share.shape[0] != counts[ctx.rank]:
+        raise ValueError("rank %d holds %d projections, expected %d" % (ctx.rank, proj_share.shape[0],
+                                                                       counts[ctx.rank]))
+    filtered = torch.as_tensor(filter_fn(proj_share))
+    everything = _all_gather_uneven(ctx, filtered, counts)  # the one exchange step
+    z0, z1 = slice_range(nz, ctx.rank, ctx.world)
+    # this rank's slices: the same z values as the whole region's z0 .. z1 - 1
+    local = backproject_fn(everything, (start + z0 * step, start + (z1 - 0.5) * step, step)) if z1 > z0 else None
+    if not gather or ctx.group is None:
+        return z0, z1, local
+    dev = ctx.device if ctx.group.get_backend() == "nccl" else "cpu"
+    t = torch.as_tensor(local).contiguous().to(dev) if local is not None else None
+    shapes = [None] * ctx.world
+    ctx.group.all_gather_object(shapes, tuple(t.shape) if t is not None else None)
+    if ctx.rank == 0:
+        parts = [t] if t is not None else []
+        for r in range(1, ctx.world):
+            if shapes[r] is None:
+                continue
+            buf = torch.empty(shapes[r], dtype=t.dtype if t is not None else torch.float32, device=dev)
+            ctx.group.recv(buf, src=r)
+            parts.append(buf)
+        return 0, nz, torch.cat(parts).cpu()
+    if t is not None:
+        ctx.group.send(t, dst=0)
+    return z0, z1, None
