@@ -274,3 +274,22 @@ def test_fused_rejections(cuda):
         f.process_projections(_t(data), ffc=ffc, dark=_t(dark), flat=_t(flat), first_row=2, n_rows=2)
     with pytest.raises(ValueError):
         f.process_projections(_t(data), ffc=ffc)  # dark and flat missing
+
+
+def test_volume_sharded_single_rank_on_gpu(cuda):
+    """reconstruct_volume_sharded with the engine's own filter and general backprojector (one
+    process: the exchange is the identity) equals the direct FDK chain."""
+    from ufob import dist as udist
+    rng = np.random.default_rng(17)
+    N, H, W = 24, 16, 64
+    proj = rng.uniform(0, 1, (N, H, W)).astype(np.float32)
+    geom = {"source-position-y": -150.0, "detector-position-y": 50.0, "center-position-x": W / 2,
+            "center-position-z": H / 2}
+    cone = dict(center_position_x=W / 2, center_position_z=H / 2, source_distance=150.0, detector_distance=50.0)
+    f = ufob.FilterTask()
+    filt = lambda p: f.process_projections(p, cone=ufob.ConeBeamProjectionWeightTask(**cone), sinograms=False)
+    bp = lambda allp, reg: ufob.GeneralBackprojectTask(num_projections=N, region=reg, **geom).process(allp)
+    z0, z1, vol = udist.reconstruct_volume_sharded(udist.Ctx(), _t(proj), N, (-4.0, 4.0, 1.0), filt, bp)
+    ref = bp(filt(_t(proj)), (-4.0, 4.0, 1.0))
+    assert (z0, z1) == (0, 8)
+    assert torch.equal(vol, ref)
