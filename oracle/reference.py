@@ -3,8 +3,8 @@
 ``_ref/libufo_ref.so`` (built by ``make -f ref.mk`` from the reference sources)
 holds the reference's own ``filter`` and ``backproject`` task code
 (src/ufo-filter-task.c, src/ufo-backproject-task.c) and its OpenCL kernels
-(src/kernels/backproject.cl, filter.cl, fft.cl, forwardproject.cl) compiled for
-the CPU against small GLib/OpenCL/ufo-core shims.  The FFT library the
+(src/kernels/backproject.cl, filter.cl, fft.cl, forwardproject.cl, ffc.cl,
+conebeam.cl) compiled for the CPU against small GLib/OpenCL/ufo-core shims.  The FFT library the
 reference calls (vendored oclfft or clFFT) is replaced by an FP64 FFT.
 
 Used to pin the FP64 oracle (oracle.py) and to generate the golden fixtures
@@ -51,6 +51,8 @@ def lib():
         L.ref_fft_pack.argtypes = [vp, vp, i, i, i, f]
         L.refshim_fft.argtypes = [vp, ctypes.c_size_t, ctypes.c_size_t, i]
         L.ref_forwardproject.argtypes = [vp, i, i, f, f, vp]
+        L.ref_flat_correct.argtypes = [vp, vp, vp, vp, i, i, i, i, i, f, f]
+        L.ref_weight_projection.argtypes = [vp, vp, i, i, f, f, f, f, f, f]
         _LIB = L
     return _LIB
 
@@ -126,4 +128,30 @@ def forwardproject(slice_img, n_angles, axis_pos, angle_step):
     W = img.shape[-1]
     out = np.zeros((n_angles, W), dtype=np.float32)
     lib().ref_forwardproject(_p(img), W, n_angles, axis_pos, angle_step, _p(out))
+    return out
+
+
+def flat_field_correct(data, dark, flat, absorption_correct=False, fix_nan_and_inf=False, sinogram_input=False,
+                       dark_scale=1.0, flat_scale=1.0):
+    """src/kernels/ffc.cl on each frame [H, W] of data [..., H, W]."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    dark = np.ascontiguousarray(dark, dtype=np.float32)
+    flat = np.ascontiguousarray(flat, dtype=np.float32)
+    H, W = data.shape[-2:]
+    frames = data.reshape(-1, H, W)
+    out = np.empty_like(frames)
+    for i in range(frames.shape[0]):
+        fr = np.ascontiguousarray(frames[i])
+        lib().ref_flat_correct(_p(out[i]), _p(fr), _p(dark), _p(flat), W, H, int(sinogram_input),
+                               int(absorption_correct), int(fix_nan_and_inf), float(dark_scale), float(flat_scale))
+    return out.reshape(data.shape)
+
+
+def weight_projection(proj, cx, cz, sd, od, mr, cs):
+    """src/kernels/conebeam.cl on one projection [H, W] with the task's FP32 kernel arguments."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    H, W = proj.shape
+    out = np.empty_like(proj)
+    lib().ref_weight_projection(_p(proj), _p(out), W, H, float(cx), float(cz), float(sd), float(od), float(mr),
+                                float(cs))
     return out

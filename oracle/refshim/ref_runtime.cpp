@@ -57,6 +57,9 @@ void filter(float *, float *, float *);
 void fft_spread(float *, float *, int, int, int);
 void fft_pack(float *, float *, int, int, float, int);
 void forwardproject(image2d_t, float *, float, float);
+void flat_correct(float *, float *, const float *, const float *, const int, const int, const int, const float,
+                  const float);
+void weight_projection(float *, float *, const float2, const float, const float, const float, const float);
 }
 
 template <typename T> static T arg(refshim_kernel *k, int i) { return *reinterpret_cast<T *>(k->args[i]); }
@@ -329,6 +332,27 @@ void ref_fft_pack(float *in, float *out, int out_width, int height, int nfft, fl
     clSetKernelArg(&k, 5, sizeof(int), &is_complex);
     gsize g[3] = {(gsize)nfft, (gsize)height, 1};
     refshim_dispatch(&k, 3, g);
+}
+
+// ffc.cl over one frame of width x height (src/ufo-flat-field-correct-task.c:150-166 launches
+// it on the frame's requisition).
+void ref_flat_correct(float *out, float *data, const float *dark, const float *flat, int width, int height,
+                      int sinogram_input, int absorptivity, int fix_abnormal, float dark_scale, float flat_scale)
+{
+    gsize g[2] = {(gsize)width, (gsize)height};
+    ndrange(2, g, [&] {
+        flat_correct(out, data, dark, flat, sinogram_input, absorptivity, fix_abnormal, dark_scale, flat_scale);
+    });
+}
+
+// conebeam.cl over one projection with the kernel arguments the task computes
+// (src/ufo-cone-beam-projection-weight-task.c:128-146).
+void ref_weight_projection(float *proj, float *out, int width, int height, float cx, float cz, float sd, float od,
+                           float mr, float cs)
+{
+    gsize g[2] = {(gsize)width, (gsize)height};
+    const float2 c = make_float2(cx, cz);
+    ndrange(2, g, [&] { weight_projection(proj, out, c, sd, od, mr, cs); });
 }
 
 // forwardproject.cl over a slice image (src/ufo-forwardproject-task.c launches

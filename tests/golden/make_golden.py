@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
 The reference's `filter` and `backproject` task sources and its OpenCL kernels
-are compiled for the CPU by oracle/ref.mk (oracle/_ref/libufo_ref.so, see
+(with the flat-field and cone-beam weight kernels) are compiled for the CPU by oracle/ref.mk (oracle/_ref/libufo_ref.so, see
 oracle/reference.py); this script runs them on seeded inputs and stores inputs
 and outputs.  Run it where the reference sources are present:
 
@@ -54,6 +54,36 @@ def main():
     out["fp_input"] = img
     out["fp_output"] = reference.forwardproject(img, 30, 32.0, math.pi / 30)
     path = os.path.join(HERE, "reference_fbp.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+    pre_golden()
+
+
+FFC_CASES = [dict(), dict(absorption_correct=True), dict(absorption_correct=True, fix_nan_and_inf=True),
+             dict(dark_scale=0.5, flat_scale=1.5)]
+CONE_CASES = [dict(center_position_x=20.5, center_position_z=9.0, source_distance=300.0, detector_distance=100.0),
+              dict(center_position_x=17.25, center_position_z=11.5, source_distance=150.0, detector_distance=60.0,
+                   axis_angle_x=0.4)]
+
+
+def pre_golden():
+    """flat-field-correct and cone-beam-projection-weight kernels of the reference (ffc.cl,
+    conebeam.cl) on seeded frames; the cone arguments are the task's FP32 host arithmetic."""
+    rng = np.random.default_rng(77)
+    H, W = 12, 40
+    dark = rng.uniform(90, 110, (H, W)).astype(np.float32)
+    flat = (dark + rng.uniform(800, 1200, (H, W))).astype(np.float32)
+    data = (dark + rng.uniform(50, 1000, (3, H, W))).astype(np.float32)
+    data[0, 0, :3] = dark[0, :3]  # zero transmission
+    out = {"ffc_dark": dark, "ffc_flat": flat, "ffc_data": data}
+    for i, c in enumerate(FFC_CASES):
+        out["ffc_%d" % i] = reference.flat_field_correct(data, dark, flat, **c)
+    proj = rng.standard_normal((H, W)).astype(np.float32)
+    out["cone_input"] = proj
+    for i, c in enumerate(CONE_CASES):
+        cx, cz, sd, od, mr, cs = oracle.cone_weight_params(0, **c)
+        out["cone_%d" % i] = reference.weight_projection(proj, cx, cz, sd, od, mr, cs)
+    path = os.path.join(HERE, "reference_pre.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")
 

@@ -293,3 +293,22 @@ def test_volume_sharded_single_rank_on_gpu(cuda):
     ref = bp(filt(_t(proj)), (-4.0, 4.0, 1.0))
     assert (z0, z1) == (0, 8)
     assert torch.equal(vol, ref)
+
+
+def test_engine_matches_reference_kernel_fixtures(cuda):
+    """The engine's flat-field correction and cone-beam weight against the outputs of the
+    reference's own ffc.cl / conebeam.cl (compiled for the CPU, tests/golden/reference_pre.npz)."""
+    import os
+    from test_oracle_pinned_pre import CONE_CASES, FFC_CASES
+    G = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_pre.npz"))
+    for i, c in enumerate(FFC_CASES):
+        props = {k: int(v) if isinstance(v, bool) else v for k, v in c.items()}
+        got = ufob.FlatFieldCorrectTask(**props).process(_t(G["ffc_data"]), _t(G["ffc_dark"]),
+                                                         _t(G["ffc_flat"])).cpu().numpy()
+        ref = G["ffc_%d" % i]
+        fin = np.isfinite(ref)
+        np.testing.assert_array_equal(np.isfinite(got), fin)
+        np.testing.assert_allclose(got[fin], ref[fin], rtol=3e-7, atol=1e-7)
+    for i, c in enumerate(CONE_CASES):
+        got = ufob.ConeBeamProjectionWeightTask(**c).process(_t(G["cone_input"])).cpu().numpy()
+        np.testing.assert_allclose(got, G["cone_%d" % i], rtol=3e-7, atol=1e-7)
