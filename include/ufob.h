@@ -253,6 +253,10 @@ void ufob_fbp_destroy(ufob_fbp *fbp);
 typedef struct ufob_gbp ufob_gbp;
 ufob_status ufob_gbp_create(ufob_gbp **out);
 ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double value);
+/* String properties as the reference's enums (parameter, compute-type, result-type, store-type,
+ * addressing-mode), plus the engine property "interpolation": "exact" (default, FP32 weights)
+ * or "texture" (the texture unit's linear filter with 8-bit weights, as the reference samples
+ * on a GPU; FP32 compute type). */
 ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value);
 ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n);
 /* setup(): validates num-projections, gray mapping; builds angle tables. */

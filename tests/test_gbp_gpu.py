@@ -205,3 +205,20 @@ def test_setup_errors(cuda):
     t.set_property("center-position-x", [1.0, 2.0, 3.0])
     with pytest.raises(ufob.UfobError):
         t.setup()
+
+
+@pytest.mark.parametrize("name", ["cone", "parallel", "lamino"])
+def test_hardware_interpolation_mode(cuda, name):
+    """interpolation=texture (engine property): the texture unit's linear filter with 8-bit
+    weights, as the reference samples on a GPU.  Close to the exact-weight result (the weights
+    differ by up to 1/512), and the default stays exact."""
+    props = dict(BASE, **GEOMETRIES[name])
+    proj = _proj(21, smooth=True)
+    exact = run_gbp(proj, props).cpu().numpy()
+    hw = run_gbp(proj, props, interpolation="texture").cpu().numpy()
+    ref = oracle_gbp(proj, props)
+    assert oracle.rel_l2(exact, ref) < 2e-5
+    assert 1e-6 < oracle.rel_l2(hw, ref) < 1e-2
+    t = ufob.GeneralBackprojectTask(num_projections=proj.shape[0])
+    with pytest.raises(ufob.UfobError):
+        t.set_property("interpolation", "cubic")

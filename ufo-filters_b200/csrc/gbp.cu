@@ -368,9 +368,10 @@ struct GBPArgs {
     int addr;
     void *vol;
     const cudaTextureObject_t *tex;  // one per projection (FP32 compute type), or null: global loads
+    int hw_interp;                   // 1: the texture unit's linear filter (8-bit weights) samples
 };
 
-template <bool CONE, typename CT, int RT, bool PARAMZ, int ZT, bool TEX>
+template <bool CONE, typename CT, int RT, bool PARAMZ, int ZT, bool TEX, bool HW = false>
 __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
 {
     constexpr int PB = 16;  // projections per staged table block
@@ -438,7 +439,8 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
                         wgt = cc * cc;
                     }
                 }
-                const float val = TEX ? bilinear_tex(tx, (int)a.W, (int)a.H, (float)u, (float)v)
+                const float val = TEX ? (HW ? tex2D<float>(tx, (float)u, (float)v)
+                                            : bilinear_tex(tx, (int)a.W, (int)a.H, (float)u, (float)v))
                                   : sizeof(CT) == 4 ? bilinear_fast(img, (int)a.W, (int)a.H, (float)u, (float)v, a.addr)
                                                     : bilinear<CT>(img, (int)a.W, (int)a.H, u, v, a.addr);
                 result_add<RT, CT>(bsum[k], CONE ? (CT)val * wgt : (CT)val);
@@ -468,7 +470,9 @@ static ufob_status launch_gbp_t(const GBPArgs &a, cudaStream_t s)
     // x/y work worth sharing), 4 otherwise (fewer detector rows per warp); measured on B200
     constexpr int ZT = PARAMZ ? (CONE ? 8 : 4) : 1;
     dim3 grid((a.nx + 31) / 32, (a.ny + 7) / 8, (a.nz + ZT - 1) / ZT);
-    if (a.tex)
+    if (a.tex && a.hw_interp)
+        k_gbp<CONE, CT, RT, PARAMZ, ZT, true, true><<<grid, 256, 0, s>>>(a);
+    else if (a.tex)
         k_gbp<CONE, CT, RT, PARAMZ, ZT, true><<<grid, 256, 0, s>>>(a);
     else
         k_gbp<CONE, CT, RT, PARAMZ, ZT, false><<<grid, 256, 0, s>>>(a);
@@ -552,6 +556,7 @@ struct ufob_gbp {
     double overall_angle = 2 * M_PI;
     int addressing_mode = AD_CLAMP;
     double gray_map_min = 0.0, gray_map_max = 0.0;
+    int interpolation = 0;  // engine property: 0 exact FP32 weights, 1 the texture unit's linear filter
     // device state
     DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol;
     uint32_t pushed = 0, pw = 0, ph = 0;
@@ -561,7 +566,7 @@ struct ufob_gbp {
     DevBuf d_tex;
     const float *tex_base = nullptr;
     uint32_t tex_w = 0, tex_h = 0;
-    int tex_addr = -1;
+    int tex_addr = -1, tex_filter = -1;
     ufob_gbp()
     {
         for (int i = 0; i < GC_NCOLS; i++) geom[i] = {0.0};
@@ -580,9 +585,10 @@ struct ufob_gbp {
 // bytes), border or clamp addressing, point sampling (the gather path).
 // Returns false when the stack does not meet the texture alignment rules.
 static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H, uint32_t n, int addr,
-                         cudaStream_t s)
+                         cudaStream_t s, int linear = 0)
 {
-    if (g->tex_base == base && g->tex_w == W && g->tex_h == H && g->tex.size() == n && g->tex_addr == addr)
+    if (g->tex_base == base && g->tex_w == W && g->tex_h == H && g->tex.size() == n && g->tex_addr == addr &&
+        g->tex_filter == linear)
         return true;
     g->drop_textures();
     int dev = 0, align = 0, palign = 0, maxw = 0, maxh = 0;
@@ -598,7 +604,7 @@ static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H,
         return false;
     cudaTextureDesc td = {};
     td.addressMode[0] = td.addressMode[1] = addr == AD_CLAMP ? cudaAddressModeBorder : cudaAddressModeClamp;
-    td.filterMode = cudaFilterModePoint;
+    td.filterMode = linear ? cudaFilterModeLinear : cudaFilterModePoint;
     td.readMode = cudaReadModeElementType;
     td.normalizedCoords = 0;
     g->tex.reserve(n);
@@ -628,6 +634,7 @@ static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H,
     g->tex_w = W;
     g->tex_h = H;
     g->tex_addr = addr;
+    g->tex_filter = linear;
     return true;
 }
 
@@ -712,6 +719,10 @@ extern "C" ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *nam
     } else if (name_is(name, "addressing-mode")) {
         if ((i = lookup(value, kAddrNames, 5)) < 0) return fail(UFOB_ERR_INVALID, "unknown addressing-mode '%s'", value);
         g->addressing_mode = i;
+    } else if (name_is(name, "interpolation")) {  // engine property
+        static const char *const kInterp[] = {"exact", "texture"};
+        if ((i = lookup(value, kInterp, 2)) < 0) return fail(UFOB_ERR_INVALID, "unknown interpolation '%s'", value);
+        g->interpolation = i;
     } else {
         char *end = nullptr;
         double v = value ? strtod(value, &end) : 0.0;
@@ -851,6 +862,7 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
     a.addr = g->addressing_mode == AD_CLAMP ? AD_CLAMP : AD_CLAMP_TO_EDGE;  // "none": defined as clamp-to-edge
     a.vol = d_vol;
     a.tex = nullptr;
+    a.hw_interp = 0;
     const bool cone = !parallel;
     if (g->compute_type == 1) {
         a.tab = g->d_tab_d.ptr;
@@ -858,7 +870,12 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
                     : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
     }
     a.tab = g->d_tab_f.ptr;
-    if (gbp_textures(g, d_proj, W, H, n, a.addr, s)) a.tex = g->d_tex.as<cudaTextureObject_t>();
+    if (gbp_textures(g, d_proj, W, H, n, a.addr, s, g->interpolation)) {
+        a.tex = g->d_tex.as<cudaTextureObject_t>();
+        a.hw_interp = g->interpolation;
+    } else if (g->interpolation) {
+        return fail(UFOB_ERR_UNSUPPORTED, "interpolation=texture needs texture-compatible projections");
+    }
     return cone ? launch_gbp_rt<true, float>(a, g->result_type, paramz, s)
                 : launch_gbp_rt<false, float>(a, g->result_type, paramz, s);
 }
@@ -1143,6 +1160,7 @@ static ufob_status lamino_compute(ufob_lamino *l, const float *d_proj, uint32_t 
     a.addr = l->addressing_mode == AD_CLAMP ? AD_CLAMP : AD_CLAMP_TO_EDGE;
     a.vol = d_vol;
     a.tex = nullptr;
+    a.hw_interp = 0;
     if (gbp_textures(&g, d_proj, W, H, n, a.addr, s)) a.tex = g.d_tex.as<cudaTextureObject_t>();
     return launch_gbp_rt<false, float>(a, RT_FLOAT, paramz, s);
 }

@@ -11,7 +11,9 @@
   200 px behind it), laminography (axis tilted by 30 degrees about x,
   `axis-angle-x` = pi/6, 0 = tomography) and the parallel-beam case through the
   same task; inputs are uniform random projections (throughput does not depend
-  on the values).
+  on the values).  Each with exact FP32 interpolation weights (the default) and
+  with the engine's `interpolation=texture` (the texture unit's linear filter,
+  8-bit weights, as the reference samples on a GPU).
 * uneven batch: 64 parallel-beam jobs with widths drawn from
   {256, 512, 1024, 1536, 2048} and 180..1800 angles (seeded), filtered and
   backprojected by one persistent launch pair captured in a CUDA graph, for
@@ -58,7 +60,7 @@ def _timeit(fn, reps):
     return a.elapsed_time(b) / reps
 
 
-def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512):
+def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "texture")):
     import torch
     from . import GeneralBackprojectTask
     proj = torch.rand(n_proj, det, det, device="cuda")
@@ -66,8 +68,9 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512):
              "lamino_30deg": {"axis-angle-x": math.pi / 6},
              "parallel": {}}
     out = []
-    for name, g in geoms.items():
+    for (name, g), interp in [(gi, ip) for ip in interpolations for gi in geoms.items()]:
         t = GeneralBackprojectTask(num_projections=n_proj)
+        t.set_property("interpolation", interp)
         t.set_property("center-position-x", det / 2.0)
         t.set_property("center-position-z", det / 2.0)
         half = vol / 2.0
@@ -80,7 +83,7 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512):
         ms = _timeit(lambda: t.process(proj, out=v), reps)
         upd = float(vol) ** 3 * n_proj
         out.append({"workload": "general-backproject %s, %d projections of %d^2 -> %d^3" % (name, n_proj, det, vol),
-                    "ms": round(ms, 2), "gups": round(upd / ms / 1e6, 1)})
+                    "interpolation": interp, "ms": round(ms, 2), "gups": round(upd / ms / 1e6, 1)})
     return out
 
 
