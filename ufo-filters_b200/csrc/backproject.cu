@@ -211,6 +211,38 @@ __device__ __forceinline__ void fma2(float &a0, float &a1, float k, float x0, fl
         : "f"(x0), "f"(x1), "f"(k));
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic; each lane rounds exactly as the
+// scalar instruction does, so the packed chains below are bit-identical to
+// their scalar forms).
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi)
+{
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(uint64_t v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c)
+{
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ uint64_t f2add(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b)
+{
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 // acc += w_lo * s_lo + w_hi * s_hi with 16-bit operands and FP32 accumulation
 // (sm_100 mixed-precision fma.rn.f32.{f16,bf16}; the products are exact in FP32).
 template <int KIND>
@@ -227,6 +259,53 @@ __device__ __forceinline__ float pair_fma(uint32_t pair, uint32_t wts, float acc
             : "+f"(acc)
             : "r"(pair), "r"(wts));
     return acc;
+}
+
+// Weights of two pixels at once: wlo = (1 - w0, 1 - w1), whi = (w0, w1) with
+// w = d + 0.5, each lane rounded once as in pair_weights.
+template <int KIND>
+__device__ __forceinline__ void pair_weights2(float d0, float d1, uint32_t &wlo, uint32_t &whi)
+{
+    if (KIND == SINO_F16_PAIRS)
+        asm("{\n\t.reg .b32 dd;\n\tcvt.rn.f16x2.f32 dd, %3, %2;\n\t"
+            "fma.rn.f16x2 %0, dd, %4, %6;\n\tfma.rn.f16x2 %1, dd, %5, %6;\n\t}"
+            : "=r"(wlo), "=r"(whi)
+            : "f"(d0), "f"(d1), "r"(0xBC00BC00u), "r"(0x3C003C00u), "r"(0x38003800u));
+    else
+        asm("{\n\t.reg .b32 dd;\n\tcvt.rn.bf16x2.f32 dd, %3, %2;\n\t"
+            "fma.rn.bf16x2 %0, dd, %4, %6;\n\tfma.rn.bf16x2 %1, dd, %5, %6;\n\t}"
+            : "=r"(wlo), "=r"(whi)
+            : "f"(d0), "f"(d1), "r"(0xBF80BF80u), "r"(0x3F803F80u), "r"(0x3F003F00u));
+}
+
+// acc += wlo[L] * s_lo + whi[L] * s_hi (lane L of the two weight pairs); same
+// products and order as pair_fma.
+template <int KIND, int L>
+__device__ __forceinline__ void pair_fma_lanes(uint32_t pair, uint32_t wlo, uint32_t whi, float &acc)
+{
+    if (KIND == SINO_F16_PAIRS) {
+        if (L == 0)
+            asm("{\n\t.reg .b16 l, h, a, b, x;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {a, x}, %2;\n\tmov.b32 {b, x}, %3;\n\t"
+                "fma.rn.f32.f16 %0, a, l, %0;\n\tfma.rn.f32.f16 %0, b, h, %0;\n\t}"
+                : "+f"(acc)
+                : "r"(pair), "r"(wlo), "r"(whi));
+        else
+            asm("{\n\t.reg .b16 l, h, a, b, x;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {x, a}, %2;\n\tmov.b32 {x, b}, %3;\n\t"
+                "fma.rn.f32.f16 %0, a, l, %0;\n\tfma.rn.f32.f16 %0, b, h, %0;\n\t}"
+                : "+f"(acc)
+                : "r"(pair), "r"(wlo), "r"(whi));
+    } else {
+        if (L == 0)
+            asm("{\n\t.reg .b16 l, h, a, b, x;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {a, x}, %2;\n\tmov.b32 {b, x}, %3;\n\t"
+                "fma.rn.f32.bf16 %0, a, l, %0;\n\tfma.rn.f32.bf16 %0, b, h, %0;\n\t}"
+                : "+f"(acc)
+                : "r"(pair), "r"(wlo), "r"(whi));
+        else
+            asm("{\n\t.reg .b16 l, h, a, b, x;\n\tmov.b32 {l, h}, %1;\n\tmov.b32 {x, a}, %2;\n\tmov.b32 {x, b}, %3;\n\t"
+                "fma.rn.f32.bf16 %0, a, l, %0;\n\tfma.rn.f32.bf16 %0, b, h, %0;\n\t}"
+                : "+f"(acc)
+                : "r"(pair), "r"(wlo), "r"(whi));
+    }
 }
 
 // Shared-memory carve-up of one backprojection CTA.
@@ -301,6 +380,10 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
     float by[RY];
 #pragma unroll
     for (int j = 0; j < RY; j++) by[j] = (float)(args.roi_y + y0 + ly + j * YSTEP) - axis + 0.5f;
+    constexpr bool PACK = ZT == 1 && RY % 2 == 0;
+    uint64_t by2[RY / 2 > 0 ? RY / 2 : 1];
+#pragma unroll
+    for (int j = 0; j + 1 < RY; j += 2) by2[j / 2] = f2pack(by[j], by[j + 1]);
 
     float acc[RY][ZT], comp[RY][ZT];
 #pragma unroll
@@ -328,7 +411,48 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
 #pragma unroll
             for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
 
-        if (ok) {
+        if (ok && PACK) {
+            // single slice: the coordinate chain of two output rows runs as packed
+            // FP32 pairs, halving the per-update arithmetic that a slice stack
+            // would otherwise share
+            const uint64_t magic2 = f2pack(kMagic, kMagic), half2 = f2pack(0.5f, 0.5f);
+#pragma unroll 2
+            for (int a = 0; a < nval; a++) {
+                const float2 sc = __ldg(&args.sincos[p0 + a]);
+                const int xs = win[slot * A + a];
+                const float t = fmaf(bx, sc.y, eoff - (float)xs);
+                const uint64_t s2 = f2pack(sc.x, sc.x), t2 = f2pack(t, t);
+                const uint32_t *row = sdata + a * ASTR;
+#pragma unroll
+                for (int j = 0; j < RY; j += 2) {
+                    const uint64_t vv = f2fma(by2[j / 2], s2, t2);
+                    const uint64_t r = f2add(vv, magic2);
+                    const uint64_t d = f2sub(vv, f2sub(r, magic2));
+                    float r0, r1;
+                    f2unpack(r, r0, r1);
+                    uint32_t e0 = (uint32_t)(__float_as_int(r0) - kMagicBits);
+                    uint32_t e1 = (uint32_t)(__float_as_int(r1) - kMagicBits);
+                    if (PAIRS) {
+                        float d0, d1;
+                        f2unpack(d, d0, d1);
+                        e0 = min(e0, (uint32_t)(WIN - 1));
+                        e1 = min(e1, (uint32_t)(WIN - 1));
+                        uint32_t wlo, whi;
+                        pair_weights2<KIND>(d0, d1, wlo, whi);
+                        pair_fma_lanes<KIND, 0>(row[e0], wlo, whi, part[j][0]);
+                        pair_fma_lanes<KIND, 1>(row[e1], wlo, whi, part[j + 1][0]);
+                    } else {
+                        const uint64_t w = f2add(d, half2), omw = f2sub(half2, d);
+                        e0 = min(e0, (uint32_t)(WIN - 2));
+                        e1 = min(e1, (uint32_t)(WIN - 2));
+                        uint64_t pp = f2pack(part[j][0], part[j + 1][0]);
+                        pp = f2fma(omw, f2pack(__uint_as_float(row[e0]), __uint_as_float(row[e1])), pp);
+                        pp = f2fma(w, f2pack(__uint_as_float(row[e0 + 1]), __uint_as_float(row[e1 + 1])), pp);
+                        f2unpack(pp, part[j][0], part[j + 1][0]);
+                    }
+                }
+            }
+        } else if (ok) {
 #pragma unroll 2
             for (int a = 0; a < nval; a++) {
                 const float2 sc = __ldg(&args.sincos[p0 + a]);
@@ -877,7 +1001,7 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
 
 // Tile-shape variants of the persistent batch kernel (single slices, ZT = 1):
 // (tile height, angles per stage).  The autotuner picks one per batch.
-static const int kBatchVariants[][2] = {{16, 32}, {32, 16}, {8, 32}, {16, 16}};
+static const int kBatchVariants[][2] = {{16, 32}, {32, 16}, {8, 32}, {16, 16}, {64, 16}, {64, 32}, {128, 16}, {96, 16}};
 
 int bp_batch_variants() { return (int)(sizeof(kBatchVariants) / sizeof(kBatchVariants[0])); }
 
@@ -895,7 +1019,11 @@ void bp_batch_tile(int v, int *tx, int *ty, int *window)
     case 0: *window = batch_window<16, 32>(); break;
     case 1: *window = batch_window<32, 16>(); break;
     case 2: *window = batch_window<8, 32>(); break;
-    default: *window = batch_window<16, 16>(); break;
+    case 3: *window = batch_window<16, 16>(); break;
+    case 4: *window = batch_window<64, 16>(); break;
+    case 5: *window = batch_window<64, 32>(); break;
+    case 6: *window = batch_window<128, 16>(); break;
+    default: *window = batch_window<96, 16>(); break;
     }
 }
 
@@ -925,6 +1053,10 @@ static ufob_status batch_variant(int v, const BatchBP *j, const uint2 *it, uint3
     case 1: return launch_batch_t<32, 16, KIND, KAHAN>(j, it, n, c, s);
     case 2: return launch_batch_t<8, 32, KIND, KAHAN>(j, it, n, c, s);
     case 3: return launch_batch_t<16, 16, KIND, KAHAN>(j, it, n, c, s);
+    case 4: return launch_batch_t<64, 16, KIND, KAHAN>(j, it, n, c, s);
+    case 5: return launch_batch_t<64, 32, KIND, KAHAN>(j, it, n, c, s);
+    case 6: return launch_batch_t<128, 16, KIND, KAHAN>(j, it, n, c, s);
+    case 7: return launch_batch_t<96, 16, KIND, KAHAN>(j, it, n, c, s);
     default: return fail(UFOB_ERR_INVALID, "backproject batch: unknown variant %d", v);
     }
 }
