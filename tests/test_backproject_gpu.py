@@ -56,7 +56,7 @@ def test_stack(cuda, nz):
         assert oracle.rel_l2(got[z], ref[z]) < 1e-5
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 8])
 def test_tiles(cuda, tile):
     s = _sino(77, 200, seed=3, nz=9)
     bp = ufob.BackprojectTask(tile=tile, roi_width=150, roi_height=170)
