@@ -256,7 +256,9 @@ ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double value);
 /* String properties as the reference's enums (parameter, compute-type, result-type, store-type,
  * addressing-mode), plus the engine property "interpolation": "exact" (default, FP32 weights)
  * or "texture" (the texture unit's linear filter with 8-bit weights, as the reference samples
- * on a GPU; FP32 compute type). */
+ * on a GPU; FP32 compute type).  compute-type "half" stores the projection samples as FP16
+ * (texture gathers of 16-bit texels run at twice the FP32 rate) and keeps coordinates, weights
+ * and sums in FP32; the reference's half type also computes those in half precision. */
 ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value);
 ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n);
 /* setup(): validates num-projections, gray mapping; builds angle tables. */

@@ -222,3 +222,39 @@ def test_hardware_interpolation_mode(cuda, name):
     t = ufob.GeneralBackprojectTask(num_projections=proj.shape[0])
     with pytest.raises(ufob.UfobError):
         t.set_property("interpolation", "cubic")
+
+
+@pytest.mark.parametrize("name", ["cone", "parallel", "lamino", "cone_lamino", "detector_tilt"])
+def test_compute_half(cuda, name):
+    """compute-type half: projection samples stored as FP16 (texture gathers of 16-bit texels),
+    coordinates, weights and sums in FP32.  Equal to the FP32 path on FP16-rounded projections."""
+    props = dict(BASE, **GEOMETRIES[name])
+    proj = _proj(31, smooth=True)
+    got = run_gbp(proj, props, **{"compute-type": "half"}).cpu().numpy()
+    rounded = proj.astype(np.float16).astype(np.float32)
+    assert oracle.rel_l2(got, oracle_gbp(rounded, props)) < 2e-5
+    assert oracle.rel_l2(got, oracle_gbp(proj, props)) < 1e-3
+
+
+def test_compute_half_padded_rows_and_modes(cuda):
+    """Rows whose FP16 pitch needs padding to the texture pitch alignment; clamp_to_edge
+    addressing; half samples with the texture unit's linear filter; switching back to float."""
+    w = 50
+    props = {"center-position-x": w / 2, "center-position-z": H / 2, "region": (-3.0, 3.0, 1.0),
+             "source-position-y": -120.0, "detector-position-y": 40.0}
+    proj = _proj(32, w=w, smooth=False)
+    rounded = proj.astype(np.float16).astype(np.float32)
+    t = ufob.GeneralBackprojectTask(num_projections=proj.shape[0])
+    for k, v in props.items():
+        t.set_property(k, v)
+    t.set_property("compute-type", "half")
+    t.set_property("addressing-mode", "clamp_to_edge")
+    got = t.process(torch.from_numpy(proj).cuda()).cpu().numpy()
+    assert oracle.rel_l2(got, oracle_gbp(rounded, props, addressing_mode="clamp_to_edge")) < 2e-5
+    t.set_property("interpolation", "texture")
+    hw = t.process(torch.from_numpy(proj).cuda()).cpu().numpy()
+    assert oracle.rel_l2(hw, oracle_gbp(rounded, props, addressing_mode="clamp_to_edge")) < 1e-2
+    t.set_property("interpolation", "exact")
+    t.set_property("compute-type", "float")
+    full = t.process(torch.from_numpy(proj).cuda()).cpu().numpy()
+    assert oracle.rel_l2(full, oracle_gbp(proj, props, addressing_mode="clamp_to_edge")) < 2e-5

@@ -550,7 +550,7 @@ struct ufob_gbp {
     std::vector<double> region{0, 0, 0}, x_region{0, 0, 0}, y_region{0, 0, 0};
     std::vector<double> geom[GC_NCOLS];
     uint32_t num_projections = 0;
-    int compute_type = 0;  // float
+    int compute_type = 0;  // 0 float, 1 double, 2 half (FP16 projection samples, FP32 arithmetic)
     int result_type = RT_FLOAT;
     int store_type = ST_FLOAT;
     double overall_angle = 2 * M_PI;
@@ -558,15 +558,15 @@ struct ufob_gbp {
     double gray_map_min = 0.0, gray_map_max = 0.0;
     int interpolation = 0;  // engine property: 0 exact FP32 weights, 1 the texture unit's linear filter
     // device state
-    DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol;
+    DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol, d_proj16;
     uint32_t pushed = 0, pw = 0, ph = 0;
     bool volume_ready = false;
     // texture objects over the projections of the last call (rebuilt when base/shape/mode change)
     std::vector<cudaTextureObject_t> tex;
     DevBuf d_tex;
-    const float *tex_base = nullptr;
+    const void *tex_base = nullptr;
     uint32_t tex_w = 0, tex_h = 0;
-    int tex_addr = -1, tex_filter = -1;
+    int tex_addr = -1, tex_filter = -1, tex_half = -1;
     ufob_gbp()
     {
         for (int i = 0; i < GC_NCOLS; i++) geom[i] = {0.0};
@@ -581,14 +581,29 @@ struct ufob_gbp {
     ~ufob_gbp() { drop_textures(); }
 };
 
-// One 2-D texture object per projection of a [n][H][W] FP32 stack (pitch W * 4
-// bytes), border or clamp addressing, point sampling (the gather path).
-// Returns false when the stack does not meet the texture alignment rules.
-static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H, uint32_t n, int addr,
-                         cudaStream_t s, int linear = 0)
+// [n][H][W] FP32 -> [n][H][pitch] FP16 (round to nearest), planes `plane` elements apart.
+__global__ void k_proj_to_half(const float *__restrict__ in, uint32_t W, uint32_t H, uint32_t n, size_t pitch,
+                               size_t plane, __half *__restrict__ out)
+{
+    const uint64_t total = (uint64_t)n * H * W;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = (uint32_t)(i % W);
+        const uint64_t r = i / W;
+        const uint32_t y = (uint32_t)(r % H), p = (uint32_t)(r / H);
+        out[(size_t)p * plane + (size_t)y * pitch + x] = __float2half_rn(__ldg(in + i));
+    }
+}
+
+// One 2-D texture object per projection of a [n][H][W] stack: FP32 with row
+// pitch W * 4 bytes, or (half) FP16 with the given row pitch and plane size in
+// elements.  Border or clamp addressing; point sampling (the gather path) or the
+// unit's linear filter.  Returns false when the stack does not meet the texture
+// alignment rules.
+static bool gbp_textures(ufob_gbp *g, const void *base, uint32_t W, uint32_t H, uint32_t n, int addr,
+                         cudaStream_t s, int linear = 0, bool half = false, size_t pitch16 = 0, size_t plane16 = 0)
 {
     if (g->tex_base == base && g->tex_w == W && g->tex_h == H && g->tex.size() == n && g->tex_addr == addr &&
-        g->tex_filter == linear)
+        g->tex_filter == linear && g->tex_half == (int)half)
         return true;
     g->drop_textures();
     int dev = 0, align = 0, palign = 0, maxw = 0, maxh = 0;
@@ -598,8 +613,9 @@ static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H,
         cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture2DLinearWidth, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&maxh, cudaDevAttrMaxTexture2DLinearHeight, dev) != cudaSuccess)
         return false;
-    const size_t plane = (size_t)W * H * sizeof(float);
-    if (((uintptr_t)base % align) || (plane % align) || ((W * sizeof(float)) % palign) || W > (uint32_t)maxw ||
+    const size_t esize = half ? 2 : 4, pitch = half ? pitch16 * 2 : (size_t)W * 4;
+    const size_t plane = half ? plane16 * 2 : (size_t)W * H * 4;
+    if (((uintptr_t)base % align) || (plane % align) || (pitch % palign) || W > (uint32_t)maxw ||
         H > (uint32_t)maxh || W < 2 || H < 2)
         return false;
     cudaTextureDesc td = {};
@@ -611,11 +627,12 @@ static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H,
     for (uint32_t p = 0; p < n; p++) {
         cudaResourceDesc rd = {};
         rd.resType = cudaResourceTypePitch2D;
-        rd.res.pitch2D.devPtr = const_cast<float *>(base) + (size_t)p * W * H;
-        rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+        rd.res.pitch2D.devPtr = const_cast<char *>(static_cast<const char *>(base)) + (size_t)p * plane;
+        rd.res.pitch2D.desc = half ? cudaCreateChannelDescHalf() : cudaCreateChannelDesc<float>();
         rd.res.pitch2D.width = W;
         rd.res.pitch2D.height = H;
-        rd.res.pitch2D.pitchInBytes = W * sizeof(float);
+        rd.res.pitch2D.pitchInBytes = pitch;
+        (void)esize;
         cudaTextureObject_t t = 0;
         if (cudaCreateTextureObject(&t, &rd, &td, nullptr) != cudaSuccess) {
             cudaGetLastError();
@@ -635,6 +652,7 @@ static bool gbp_textures(ufob_gbp *g, const float *base, uint32_t W, uint32_t H,
     g->tex_h = H;
     g->tex_addr = addr;
     g->tex_filter = linear;
+    g->tex_half = (int)half;
     return true;
 }
 
@@ -708,8 +726,8 @@ extern "C" ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *nam
             return fail(UFOB_ERR_UNSUPPORTED, "parameter axis-angle-z (the tomographic angle) cannot be swept");
         g->parameter = i;
     } else if (name_is(name, "compute-type")) {
-        if ((i = lookup(value, kResultNames + 1, 2)) < 0) return fail(UFOB_ERR_INVALID, "unknown compute-type '%s'", value);
-        g->compute_type = i;
+        if ((i = lookup(value, kResultNames, 3)) < 0) return fail(UFOB_ERR_INVALID, "unknown compute-type '%s'", value);
+        g->compute_type = i == 0 ? 2 : i - 1;
     } else if (name_is(name, "result-type")) {
         if ((i = lookup(value, kResultNames, 3)) < 0) return fail(UFOB_ERR_INVALID, "unknown result-type '%s'", value);
         g->result_type = i;
@@ -767,6 +785,28 @@ extern "C" ufob_status ufob_gbp_get_requisition(ufob_gbp *g, uint32_t width, uin
     if (ow) *ow = w;
     if (oh) *oh = h;
     if (ns) *ns = n;
+    return UFOB_OK;
+}
+
+// FP16 copy of the projections for compute-type half, rows and planes padded to
+// the texture pitch and base alignment.
+static ufob_status half_projections(ufob_gbp *g, const float *d_proj, uint32_t W, uint32_t H, uint32_t n,
+                                    cudaStream_t s, size_t *pitch16, size_t *plane16)
+{
+    int dev = 0, align = 0, palign = 0;
+    UFOB_CUDA_TRY(cudaGetDevice(&dev));
+    UFOB_CUDA_TRY(cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev));
+    UFOB_CUDA_TRY(cudaDeviceGetAttribute(&palign, cudaDevAttrTexturePitchAlignment, dev));
+    const size_t pe = (size_t)std::max(palign, 2) / 2, ae = (size_t)std::max(align, 2) / 2;
+    *pitch16 = ((size_t)W + pe - 1) / pe * pe;
+    *plane16 = (*pitch16 * H + ae - 1) / ae * ae;
+    UFOB_TRY(g->d_proj16.ensure((size_t)n * *plane16 * sizeof(__half)));
+    const uint64_t total = (uint64_t)n * H * W;
+    if (!total) return UFOB_OK;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((total + 255) / 256, (uint64_t)num_sms() * 16);
+    k_proj_to_half<<<grid, 256, 0, s>>>(d_proj, W, H, n, *pitch16, *plane16, g->d_proj16.as<__half>());
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
     return UFOB_OK;
 }
 
@@ -870,6 +910,18 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
                     : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
     }
     a.tab = g->d_tab_f.ptr;
+    if (g->compute_type == 2) {
+        // FP16 samples: the gather unit returns 16-bit texels at twice the FP32 rate;
+        // coordinates, weights and sums stay FP32
+        size_t pitch16 = 0, plane16 = 0;
+        UFOB_TRY(half_projections(g, d_proj, W, H, n, s, &pitch16, &plane16));
+        if (!gbp_textures(g, g->d_proj16.ptr, W, H, n, a.addr, s, g->interpolation, true, pitch16, plane16))
+            return fail(UFOB_ERR_UNSUPPORTED, "compute-type half needs texture-compatible projections (%ux%u)", W, H);
+        a.tex = g->d_tex.as<cudaTextureObject_t>();
+        a.hw_interp = g->interpolation;
+        return cone ? launch_gbp_rt<true, float>(a, g->result_type, paramz, s)
+                    : launch_gbp_rt<false, float>(a, g->result_type, paramz, s);
+    }
     if (gbp_textures(g, d_proj, W, H, n, a.addr, s, g->interpolation)) {
         a.tex = g->d_tex.as<cudaTextureObject_t>();
         a.hw_interp = g->interpolation;

@@ -60,7 +60,8 @@ def _timeit(fn, reps):
     return a.elapsed_time(b) / reps
 
 
-def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "texture")):
+def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "texture"),
+              computes=("float", "half")):
     import torch
     from . import GeneralBackprojectTask
     proj = torch.rand(n_proj, det, det, device="cuda")
@@ -68,9 +69,10 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "
              "lamino_30deg": {"axis-angle-x": math.pi / 6},
              "parallel": {}}
     out = []
-    for (name, g), interp in [(gi, ip) for ip in interpolations for gi in geoms.items()]:
+    for (name, g), interp, ct in [(gi, ip, c) for c in computes for ip in interpolations for gi in geoms.items()]:
         t = GeneralBackprojectTask(num_projections=n_proj)
         t.set_property("interpolation", interp)
+        t.set_property("compute-type", ct)
         t.set_property("center-position-x", det / 2.0)
         t.set_property("center-position-z", det / 2.0)
         half = vol / 2.0
@@ -83,7 +85,8 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "
         ms = _timeit(lambda: t.process(proj, out=v), reps)
         upd = float(vol) ** 3 * n_proj
         out.append({"workload": "general-backproject %s, %d projections of %d^2 -> %d^3" % (name, n_proj, det, vol),
-                    "interpolation": interp, "ms": round(ms, 2), "gups": round(upd / ms / 1e6, 1)})
+                    "interpolation": interp, "compute_type": ct, "ms": round(ms, 2),
+                    "gups": round(upd / ms / 1e6, 1)})
     return out
 
 
