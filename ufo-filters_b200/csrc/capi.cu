@@ -813,10 +813,11 @@ extern "C" ufob_status ufob_fbp_kernel_times(ufob_fbp *x, double *filter_ms, uin
 
 static uint32_t group_slices(uint32_t width, uint32_t height, uint32_t nslices)
 {
-    // bound the filtered workspace to ~2 GiB, in multiples of 8 slices
+    // bound the filtered workspace to ~2 GiB, in multiples of 32 slices (whole slice tiles of
+    // the backprojectors, which run 4 to 32 slices per CTA) or, for very large slices, of 8
     const uint64_t per_slice = (uint64_t)(width + 4) * 4 * height;
-    uint64_t g = std::max<uint64_t>(8, (2ull << 30) / std::max<uint64_t>(per_slice, 1));
-    g = g / 8 * 8;
+    uint64_t g = (2ull << 30) / std::max<uint64_t>(per_slice, 1);
+    g = g >= 32 ? g / 32 * 32 : std::max<uint64_t>(8, g / 8 * 8);
     return (uint32_t)std::min<uint64_t>(g, nslices);
 }
 
