@@ -362,7 +362,7 @@ def main():
         e2e = {"value": nz_e2e * float(W) * W * P * world / dt / 1e9, "unit": "GUPS",
                "h2d_bytes_per_step": nz_e2e * P * W * 4, "d2h_bytes_per_step": nz_e2e * W * W * 4,
                "slices": nz_e2e, "s_per_step": dt,
-               "api": "ufob_fbp_run_host (C ABI), pinned host buffers, 64-slice chunks on two streams"}
+               "api": "ufob_fbp_run_host (C ABI), pinned host buffers, 64-slice chunks (16-slice first and last) on two streams"}
         del fbp, h_in, h_out
 
     # roofline of the dominant kernel (backprojection)

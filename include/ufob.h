@@ -224,7 +224,10 @@ void ufob_stacked_bp_destroy(ufob_stacked_bp *sb);
  * `storage` is the filtered-sinogram storage type (F32, F16 or BF16).  The
  * engine streams slice groups through its own workspace.  Host-pointer
  * variant: inputs/outputs in host memory (pinned or pageable), copies are
- * overlapped with compute on internal streams.
+ * overlapped with compute on internal streams, in chunks of slices_per_chunk
+ * slices (0 = 32); from 32 up, the first and the last chunk are 16 slices, so
+ * the first compute waits for a short upload and little download trails the
+ * last one.
  */
 typedef struct ufob_fbp ufob_fbp;
 ufob_status ufob_fbp_create(const ufob_filter_props *fprops, const ufob_bp_props *bprops, ufob_dtype storage,

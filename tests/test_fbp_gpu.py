@@ -54,6 +54,19 @@ def test_host_pipeline_matches_device(cuda):
     np.testing.assert_array_equal(dev, host)
 
 
+@pytest.mark.parametrize("nz,chunk", [(37, 32), (80, 32), (33, 64), (16, 32)])
+def test_host_pipeline_ramped_chunks(cuda, nz, chunk):
+    """From 32 slices per chunk up, the last chunk is 16 slices and, for stacks of at least
+    chunk + 32 slices, the first one too (80 with 32: 16 + 32 + 16 + 16; 37 with 32: 21 + 16).
+    The default tiles share one angle-block length, so results do not depend on the grouping."""
+    P, W = 64, 64
+    stack = np.stack([phantom_sino(70 + z, W, P)[0] for z in range(nz)])
+    fbp = ufob.FBP()
+    dev = fbp.process(torch.from_numpy(stack).cuda()).cpu().numpy()
+    host = fbp.process_host(torch.from_numpy(stack).pin_memory(), slices_per_chunk=chunk).numpy()
+    np.testing.assert_array_equal(dev, host)
+
+
 def test_reconstruction_quality(cuda):
     """FBP of an analytic single-ellipse sinogram recovers its density."""
     ell = np.array([[0.2, -0.1, 0.3, 0.2, 0.4, 1.0]])

@@ -985,7 +985,7 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
                                  uint64_t slice_pitch, float *d_out, cudaStream_t stream)
 {
     switch (tile) {
-    case 0: return launch_linear<32, 16, 1, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 0: return launch_linear<32, 16, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 1: return launch_linear<32, 32, 2, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 2: return launch_linear<32, 32, 4, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 3: return launch_linear<32, 16, 4, 16, 4, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);

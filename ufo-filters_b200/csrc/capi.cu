@@ -889,10 +889,20 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
     }
     // Pipeline: H2D(c) on the upload stream -> filter+BP(c) on the compute stream -> D2H(c) on the download
     // stream, double-buffered so chunk c+1's upload and chunk c-1's download overlap chunk c's compute.
+    // Chunk sizes: a short first chunk (compute starts after a small upload) and a short last one
+    // (little download left after the last compute), `chunk` slices in between.
+    const uint32_t edge = chunk >= 32 ? 16 : 0;
+    auto chunk_at = [&](uint32_t z) -> uint32_t {
+        const uint32_t rest = nslices - z;
+        if (edge && z == 0 && nslices >= chunk + 2 * edge) return edge;
+        if (rest > chunk + edge) return chunk;
+        if (edge && rest >= 2 * edge) return rest - edge;
+        return rest;
+    };
     uint32_t c = 0;
-    for (uint32_t z = 0; z < nslices; z += chunk, c++) {
+    for (uint32_t z = 0, nz = 0; z < nslices; z += nz, c++) {
         const int b = c & 1;
-        const uint32_t nz = std::min(chunk, nslices - z);
+        nz = chunk_at(z);
         if (c >= 2) UFOB_CUDA_TRY(cudaStreamWaitEvent(x->s_copy, x->ev_done[b], 0));  // hin[b] free again
         UFOB_CUDA_TRY(cudaMemcpyAsync(x->hin[b].ptr, h_sino + (size_t)z * width * height, (size_t)nz * width * height * 4,
                                       cudaMemcpyHostToDevice, x->s_copy));
