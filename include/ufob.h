@@ -178,9 +178,9 @@ void ufob_backproject_destroy(ufob_backproject *bp);
 
 /* Allocation-free backprojection (engine addition; it has no counterpart in
  * the reference).  For callers that cannot allocate device memory: hosts that
- * manage every byte of device memory in their own pool, acquisition pipelines
- * that must not risk the device-wide synchronisation an allocation can imply,
- * and code running while a stream is captured.  Same result as
+ * manage every byte of device memory in their own pool, and acquisition
+ * pipelines that must not risk the device-wide synchronisation an allocation
+ * can imply.  Same result as
  * ufob_backproject_run() with the same properties, but stateless and without
  * any cudaMalloc/cudaFree: the only scratch, the per-angle sin/cos table,
  * lives in a fixed device array of UFOB_STATIC_MAX_ANGLES entries (256 KiB,

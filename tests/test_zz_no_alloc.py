@@ -2,7 +2,7 @@
 ABI must give the result of ufob_backproject_run() for the same properties.
 
 It exists for callers that cannot call cudaMalloc (memory-pool hosts,
-streaming acquisition, stream capture); its only scratch is a fixed device
+streaming acquisition); its only scratch is a fixed device
 array shared by all calls, so two calls in a row with different geometry
 check that each call rewrites what it reads.  This file is collected last."""
 import ctypes

@@ -4,10 +4,9 @@
 // that the handle allocates on first use (and restages sinograms whose rows are
 // not 16-byte aligned into another allocated buffer).  Some callers cannot call
 // cudaMalloc at all: hosts that own every byte of device memory through their
-// own pool and forbid outside allocations, acquisition pipelines that must not
-// take the device-wide synchronisation an allocation can imply while frames are
-// streaming, and code that runs while a stream is being captured, where an
-// allocation call is not allowed.  For them this file provides
+// own pool and forbid outside allocations, and acquisition pipelines that must
+// not take the device-wide synchronisation an allocation can imply while frames
+// are streaming.  For them this file provides
 // ufob_backproject_run_static(): the same kernels, with the only scratch they
 // need -- the angle table -- in a fixed file-scope device array.
 //
