@@ -202,12 +202,18 @@ def main(argv=None):
     ap.add_argument("--detector", type=int, default=1024)
     ap.add_argument("--volume", type=int, default=512)
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--gbp-compute", choices=["float", "half", "both"], default="both",
+                    help="compute-type(s) of the general backprojection")
+    ap.add_argument("--gbp-interp", choices=["exact", "texture", "both"], default="both",
+                    help="interpolation mode(s) of the general backprojection")
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
     only = args.gbp or args.batch or args.pre or args.stacked or args.lamino
     if args.gbp or not only:
-        rows += bench_gbp(args.reps, args.projections, args.detector, args.volume)
+        computes = ("float", "half") if args.gbp_compute == "both" else (args.gbp_compute,)
+        interps = ("exact", "texture") if args.gbp_interp == "both" else (args.gbp_interp,)
+        rows += bench_gbp(args.reps, args.projections, args.detector, args.volume, interps, computes)
     if args.batch or not only:
         rows += bench_batch()
     if args.pre or not only:
