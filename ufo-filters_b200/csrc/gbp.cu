@@ -292,9 +292,11 @@ __device__ __forceinline__ float bilinear_tex(cudaTextureObject_t t, int W, int 
     const float M = 12582912.0f;  // 1.5 * 2^23
     u = fminf(fmaxf(u, -2.0f), (float)W + 2.0f);
     v = fminf(fmaxf(v, -2.0f), (float)H + 2.0f);
-    const float fu = (u + (M - 1.0f)) - M, fv = (v + (M - 1.0f)) - M;  // rint(u - 1) = floor(u - 0.5) but ties
-    const float a = (u - 0.5f) - fu, b = (v - 0.5f) - fv;
-    const float4 g = tex2Dgather<float4>(t, fu + 1.0f, fv + 1.0f, 0);
+    // gu = rint(u) = floor(u - 0.5) + 1 but ties: the footprint's centre; the weights
+    // a = (u + 0.5) - gu equal (u - 0.5) - floor(u - 0.5), both steps exact for |u| < 2^22
+    const float gu = (u + (M - 1.0f)) - (M - 1.0f), gv = (v + (M - 1.0f)) - (M - 1.0f);
+    const float a = (u + 0.5f) - gu, b = (v + 0.5f) - gv;
+    const float4 g = tex2Dgather<float4>(t, gu, gv, 0);
     const float top = fmaf(a, g.z - g.w, g.w), bot = fmaf(a, g.y - g.x, g.x);
     return fmaf(b, bot - top, top);
 }
