@@ -343,6 +343,10 @@ ufob_status ufob_batch_create(const ufob_filter_props *fprops, ufob_dtype storag
 ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint32_t n, void *stream);
 /* Tile-shape variant the autotuner chose for the current batch (-1 before the first run). */
 int ufob_batch_variant(ufob_batch *b);
+/* Number of tile-shape variants, and pinning one of them (0 .. count-1) in place of the
+ * autotuner (-1, the default, restores autotuning); takes effect at the next run. */
+int ufob_batch_variants(void);
+ufob_status ufob_batch_set_variant(ufob_batch *b, int variant);
 void ufob_batch_destroy(ufob_batch *b);
 
 /* ---------------------------------------------------------- preprocessing

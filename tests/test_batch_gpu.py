@@ -54,6 +54,31 @@ def test_batch_matches_oracle(cuda, storage, tol):
         assert oracle.rel_l2(j["out"].cpu().numpy(), ref) < tol
 
 
+@pytest.mark.parametrize("storage,tol", [(ufob.F32, 1e-5), (ufob.F16, 1e-3), (ufob.BF16, 8e-3)])
+def test_every_tile_variant_matches_oracle(cuda, storage, tol):
+    """Each tile shape the autotuner may pick (pinned one by one), on the uneven jobs plus a
+    1536-angle job, which turns on the blocked-Kahan sums of the 16-bit forms."""
+    jobs, refs = _jobs(4)
+    W, P = 128, 1536
+    ell = oracle.random_ellipses(4321)
+    sino = oracle.ellipse_sinogram(ell, W, np.arange(P) * math.pi / P).astype(np.float32)
+    refs.append(oracle.backproject(oracle.fft_filter_ifft(sino, size_x=W, crop_width=W).astype(np.float32)))
+    jobs.append(dict(sino=torch.from_numpy(sino).cuda(), out=torch.zeros((W, W), device="cuda")))
+    b = ufob.Batch(storage=storage)
+    assert ufob.Batch.variants() == 8
+    for v in range(ufob.Batch.variants()):
+        b.set_variant(v)
+        for j in jobs:
+            j["out"].zero_()
+        b.run(jobs)
+        torch.cuda.synchronize()
+        ufob.device_status()
+        assert b.variant() == v
+        for j, ref in zip(jobs, refs):
+            assert oracle.rel_l2(j["out"].cpu().numpy(), ref) < tol, (v, j["sino"].shape)
+    b.set_variant(-1)
+
+
 def test_batch_graph_replay_and_change(cuda):
     jobs, refs = _jobs(2)
     b = ufob.Batch()

@@ -142,3 +142,17 @@ def test_status_strings():
     L = ufob.lib()
     for s in range(8):
         assert L.ufob_status_string(s)
+
+
+def test_batch_variant_pinning_range():
+    """Tile variants can be pinned from 0 to variants()-1, or -1 for the autotuner."""
+    b = ufob.Batch()
+    n = ufob.Batch.variants()
+    assert n == 8
+    b.set_variant(n - 1)
+    b.set_variant(-1)
+    with pytest.raises(ufob.UfobError):
+        b.set_variant(n)
+    with pytest.raises(ufob.UfobError):
+        b.set_variant(-2)
+

@@ -103,6 +103,7 @@ struct ufob_batch {
     std::vector<float2 *> outs;
     std::string signature;
     int variant = -1;
+    int pinned = -1;  // tile variant fixed by ufob_batch_set_variant, -1 = autotuned
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t maxN = 0, maxP = 0;
@@ -336,8 +337,8 @@ extern "C" ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint3
             cudaGraphDestroy(b->graph);
             b->graph = nullptr;
         }
-        int v = 0;
-        UFOB_TRY(batch_autotune(b, jobs, n, s, &v));
+        int v = b->pinned;
+        if (v < 0) UFOB_TRY(batch_autotune(b, jobs, n, s, &v));
         UFOB_TRY(batch_build(b, jobs, n, v));
         // capture the whole batch (counter resets + three persistent launches) once
         cudaStream_t cap;
@@ -363,3 +364,17 @@ extern "C" ufob_status ufob_batch_run(ufob_batch *b, const ufob_job *jobs, uint3
 }
 
 extern "C" int ufob_batch_variant(ufob_batch *b) { return b ? b->variant : -1; }
+
+extern "C" int ufob_batch_variants(void) { return bp_batch_variants(); }
+
+extern "C" ufob_status ufob_batch_set_variant(ufob_batch *b, int variant)
+{
+    if (!b) return fail(UFOB_ERR_INVALID, "batch handle is NULL");
+    if (variant < -1 || variant >= bp_batch_variants())
+        return fail(UFOB_ERR_INVALID, "batch: tile variant %d outside [-1, %d]", variant, bp_batch_variants() - 1);
+    if (variant != b->pinned) {
+        b->pinned = variant;
+        b->signature.clear();  // rebuild and recapture on the next run
+    }
+    return UFOB_OK;
+}

@@ -121,6 +121,8 @@ def lib():
             "ufob_batch_run": ([vp, ctypes.POINTER(Job), u32, vp], i),
             "ufob_batch_destroy": ([vp], None),
             "ufob_batch_variant": ([vp], i),
+            "ufob_batch_variants": ([], i),
+            "ufob_batch_set_variant": ([vp, i], i),
             "ufob_phantom_sinogram": ([vp, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_phantom_stack": ([vp, u32, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_launch_count": ([], ctypes.c_uint64),
@@ -561,6 +563,15 @@ class Batch:
 
     def variant(self):
         return int(lib().ufob_batch_variant(self._h))
+
+    @staticmethod
+    def variants():
+        """Number of tile-shape variants of the batch backprojector."""
+        return int(lib().ufob_batch_variants())
+
+    def set_variant(self, v):
+        """Pin tile-shape variant v (0 .. variants()-1) instead of autotuning; -1 autotunes."""
+        check(lib().ufob_batch_set_variant(self._h, int(v)))
 
     def __del__(self):
         h, fn = getattr(self, "_h", None), getattr(self, "_destroy", None)
