@@ -56,7 +56,7 @@ def test_stack(cuda, nz):
         assert oracle.rel_l2(got[z], ref[z]) < 1e-5
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 8])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6, 7, 8])
 def test_tiles(cuda, tile):
     s = _sino(77, 200, seed=3, nz=9)
     bp = ufob.BackprojectTask(tile=tile, roi_width=150, roi_height=170)
@@ -113,3 +113,23 @@ def test_pairs_storage(cuda, dtype, tol, kahan):
     got = bp.process(pairs, dtype=dtype, layout=ufob.PAIRS, width=W).cpu().numpy()
     ref = oracle.backproject(oracle.fft_filter_ifft(raw).astype(np.float32))
     assert oracle.rel_l2(got, ref) < tol
+
+
+@pytest.mark.parametrize("dtype,tol", [(ufob.F16, 1e-3), (ufob.BF16, 8e-3)])
+@pytest.mark.parametrize("tile", [0, 8])
+@pytest.mark.parametrize("kahan", [0, 1])
+def test_pairs_single_slice_tiles(cuda, dtype, tol, tile, kahan):
+    """One 16-bit pair sinogram through both single-slice tiles (32x16 and 32x96 pixels),
+    whose coordinate chain and weight pairs run two output rows at a time."""
+    rng = np.random.default_rng(11)
+    W, P = 320, 250
+    raw = rng.standard_normal((P, W)).astype(np.float32)
+    f = ufob.FilterTask(size_x=512, crop_width=W)
+    pairs = f.process(torch.from_numpy(raw).cuda(), dtype=dtype, layout=ufob.PAIRS)
+    bp = ufob.BackprojectTask(tile=tile, compensated=kahan, roi_width=300, roi_height=290)
+    got = bp.process(pairs, dtype=dtype, layout=ufob.PAIRS, width=W).cpu().numpy()
+    ref = oracle.backproject(oracle.fft_filter_ifft(raw, size_x=512, crop_width=W).astype(np.float32),
+                             roi_width=300, roi_height=290)
+    assert got.shape == ref.shape
+    assert oracle.rel_l2(got, ref) < tol
+
