@@ -774,6 +774,14 @@ __device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPAr
     const uint32_t kFixBits = __float_as_uint(kFix);
     const float toff = axis + 0.5f;  // cell coordinate = h - 0.5 + 1 - window origin
     bool aborted = false;
+    // FP32 accumulation: partial sums run over FOLD angle blocks before they are added
+    // (compensated) into the totals
+    constexpr int FOLD = ACC == QACC_F32 ? 2 : 1;
+    float part[RY][ZT];
+#pragma unroll
+    for (int j = 0; j < RY; j++)
+#pragma unroll
+        for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
 
     for (int blk = 0; blk < nblk; blk++) {
         if (tid == 0 && blk + S - 1 < nblk) issue(blk + S - 1);
@@ -783,12 +791,6 @@ __device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPAr
         const int p0 = blk * A;
         const int nval = min(A, (int)P - p0);
         const uint32_t *sdata = data + (size_t)slot * A * ASTR;
-
-        float part[RY][ZT];
-#pragma unroll
-        for (int j = 0; j < RY; j++)
-#pragma unroll
-            for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
 
         if (ok) {
             for (int a0 = 0; a0 < nval; a0 += KB) {
@@ -839,19 +841,22 @@ __device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPAr
                 }
             }
         }
+        if ((blk + 1) % FOLD == 0 || blk + 1 == nblk) {
 #pragma unroll
-        for (int j = 0; j < RY; j++)
+            for (int j = 0; j < RY; j++)
 #pragma unroll
-            for (int z = 0; z < ZT; z++) {
-                if (KAHAN) {
-                    const float yk = part[j][z] - comp[j][z];
-                    const float tk = acc[j][z] + yk;
-                    comp[j][z] = (tk - acc[j][z]) - yk;
-                    acc[j][z] = tk;
-                } else {
-                    acc[j][z] += part[j][z];
+                for (int z = 0; z < ZT; z++) {
+                    if (KAHAN) {
+                        const float yk = part[j][z] - comp[j][z];
+                        const float tk = acc[j][z] + yk;
+                        comp[j][z] = (tk - acc[j][z]) - yk;
+                        acc[j][z] = tk;
+                    } else {
+                        acc[j][z] += part[j][z];
+                    }
+                    part[j][z] = 0.f;
                 }
-            }
+        }
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;
