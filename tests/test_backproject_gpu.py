@@ -56,7 +56,7 @@ def test_stack(cuda, nz):
         assert oracle.rel_l2(got[z], ref[z]) < 1e-5
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9])
 def test_tiles(cuda, tile):
     s = _sino(77, 200, seed=3, nz=9)
     bp = ufob.BackprojectTask(tile=tile, roi_width=150, roi_height=170)
@@ -116,10 +116,10 @@ def test_pairs_storage(cuda, dtype, tol, kahan):
 
 
 @pytest.mark.parametrize("dtype,tol", [(ufob.F16, 1e-3), (ufob.BF16, 8e-3)])
-@pytest.mark.parametrize("tile", [0, 8])
+@pytest.mark.parametrize("tile", [0, 8, 9])
 @pytest.mark.parametrize("kahan", [0, 1])
 def test_pairs_single_slice_tiles(cuda, dtype, tol, tile, kahan):
-    """One 16-bit pair sinogram through both single-slice tiles (32x16 and 32x96 pixels),
+    """One 16-bit pair sinogram through the single-slice tiles (32x16, 32x96, 32x32 pixels),
     whose coordinate chain and weight pairs run two output rows at a time."""
     rng = np.random.default_rng(11)
     W, P = 320, 250

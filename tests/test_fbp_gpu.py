@@ -45,6 +45,17 @@ def test_stack_storage(cuda, storage, tol):
     assert oracle.rel_l2(got, ref) < tol
 
 
+@pytest.mark.parametrize("storage,tol", [(ufob.F32, 1e-5), (ufob.F16, 1e-3), (ufob.BF16, 8e-3)])
+def test_single_sinogram_each_storage(cuda, storage, tol):
+    """One sinogram (the reference task's unit of work); 16-bit storage keeps it as pairs."""
+    P, W = 300, 512
+    s = phantom_sino(44, W, P)[0]
+    got = ufob.FBP(storage=storage).process(torch.from_numpy(s).cuda()).cpu().numpy()
+    ref = oracle.fbp(s[None])[0]
+    assert got.shape == ref.shape == (W, W)
+    assert oracle.rel_l2(got, ref) < tol
+
+
 def test_host_pipeline_matches_device(cuda):
     nz, P, W = 20, 128, 128
     stack = np.stack([phantom_sino(30 + z, W, P)[0] for z in range(nz)])

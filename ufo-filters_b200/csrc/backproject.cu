@@ -999,6 +999,7 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
     case 6: return launch_linear<32, 32, 8, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 7: return launch_linear<32, 16, 4, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 8: return launch_linear<32, 96, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    case 9: return launch_linear<32, 32, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     default: return fail(UFOB_ERR_INVALID, "backproject: unknown tile id %d", tile);
     }
 }
@@ -1162,10 +1163,14 @@ ufob_status bp_quads_launch(const BPGeometry &g, const void *d_sino, uint32_t pi
 
 static int default_tile(const BPGeometry &g)
 {
-    // one slice: 96-row tiles share each angle's setup across 12 rows per thread,
-    // when the slice still gives every SM two of them
-    if (g.nz == 1)
-        return (uint64_t)((g.roi_w + 31) / 32) * ((g.roi_h + 95) / 96) >= 2ull * (uint64_t)num_sms() ? 8 : 0;
+    // one slice: 96-row tiles share each angle's setup across 12 rows per thread, when the
+    // slice still gives every SM two of them; else 32-row tiles when it gives every SM one;
+    // else the 16-row tile (measured on 256^2 to 2048^2 slices)
+    if (g.nz == 1) {
+        const uint64_t tx = (g.roi_w + 31) / 32, sms = (uint64_t)num_sms();
+        if (tx * ((g.roi_h + 95) / 96) >= 2 * sms) return 8;
+        return tx * ((g.roi_h + 31) / 32) >= sms ? 9 : 0;
+    }
     if (g.nz == 2) return 1;
     return 2;
 }

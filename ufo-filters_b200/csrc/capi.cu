@@ -746,9 +746,10 @@ static ufob_status fbp_group(ufob_fbp *x, const RowSource &src, uint32_t width, 
     uint32_t nfft, fw;
     UFOB_TRY(filter_sizes(x->f->props, width, &nfft, &fw));
     UFOB_TRY(filter_plan_build(x->f->props, nfft, x->f->plan, s));
-    // F16: slice-quad cells (16 B per detector position and four slices); BF16: pairs; F32: rows
-    const bool quads = x->storage == UFOB_F16;
-    const bool pairs = x->storage == UFOB_BF16;
+    // F16: slice-quad cells (16 B per detector position and four slices), or pairs for a single
+    // slice (a quad cell would carry three empty slices); BF16: pairs; F32: rows
+    const bool quads = x->storage == UFOB_F16 && nz > 1;
+    const bool pairs = x->storage == UFOB_BF16 || (x->storage == UFOB_F16 && nz == 1);
     const uint32_t pitch = quads ? fw + 1 : pairs ? round_up(fw + 1, 4) : round_up(fw, 4);
     const size_t work_bytes = quads ? (size_t)pitch * 16 * height * ((nz + 3) / 4) : (size_t)pitch * 4 * height * nz;
     UFOB_TRY(x->work.ensure(work_bytes));

@@ -5,6 +5,7 @@
     python -m ufob.bench_configs --pre      # only the preprocessing stages
     python -m ufob.bench_configs --stacked  # only stacked-backproject
     python -m ufob.bench_configs --lamino   # only lamino-backproject
+    python -m ufob.bench_configs --single   # only the one-slice 512^2 x 512 FBP
 
 * general backprojection: 1024 projections of 1024^2 over 360 degrees into a
   512^3 volume, for the cone geometry (source 800 px before the axis, detector
@@ -87,6 +88,24 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "
         out.append({"workload": "general-backproject %s, %d projections of %d^2 -> %d^3" % (name, n_proj, det, vol),
                     "interpolation": interp, "compute_type": ct, "ms": round(ms, 2),
                     "gups": round(upd / ms / 1e6, 1)})
+    return out
+
+
+def bench_single(reps=200, seed=7, width=512, n_angles=512):
+    """One 512^2 slice from 512 angles (the reference's CPU-runnable case): the whole
+    fft ! filter ! ifft ! backproject call per slice, plain FP32 and FP16 pair storage."""
+    import torch
+    from . import F16, F32, FBP, phantom_sinogram
+    from .cnn import random_ellipses
+    sino = phantom_sinogram(random_ellipses(seed), width, n_angles)
+    out = []
+    for name, storage in (("fp32", F32), ("fp16", F16)):
+        fbp = FBP(bp_props={"axis_pos": (width - 1) / 2.0}, storage=storage)
+        img = fbp.process(sino)
+        ms = _timeit(lambda: fbp.process(sino, out=img), reps)
+        out.append({"workload": "one slice: %d px x %d angles, axis %.1f, %s storage" % (width, n_angles,
+                                                                                       (width - 1) / 2.0, name),
+                    "us_per_slice": round(ms * 1e3, 1), "gups": round(width * width * n_angles / ms / 1e6, 1)})
     return out
 
 
@@ -197,6 +216,7 @@ def main(argv=None):
     ap.add_argument("--pre", action="store_true", help="only the preprocessing stages")
     ap.add_argument("--stacked", action="store_true", help="only stacked-backproject")
     ap.add_argument("--lamino", action="store_true", help="only lamino-backproject")
+    ap.add_argument("--single", action="store_true", help="only the one-slice 512^2 x 512 FBP")
     ap.add_argument("--pre-rows", type=int, default=256, help="detector rows of the preprocessing workload")
     ap.add_argument("--projections", type=int, default=1024)
     ap.add_argument("--detector", type=int, default=1024)
@@ -209,7 +229,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
-    only = args.gbp or args.batch or args.pre or args.stacked or args.lamino
+    only = args.gbp or args.batch or args.pre or args.stacked or args.lamino or args.single
     if args.gbp or not only:
         computes = ("float", "half") if args.gbp_compute == "both" else (args.gbp_compute,)
         interps = ("exact", "texture") if args.gbp_interp == "both" else (args.gbp_interp,)
@@ -222,6 +242,8 @@ def main(argv=None):
         rows += bench_stacked()
     if args.lamino or not only:
         rows += bench_lamino()
+    if args.single or not only:
+        rows += bench_single()
     device_status()
     for r in rows:
         print(json.dumps(r))
