@@ -328,7 +328,7 @@ struct BPSmem {
 // the angle blocks this CTA has already staged through the S-slot ring, so
 // one CTA can run many tiles back to back (slot = running block % S, barrier
 // parity = (running block / S) & 1).  Returns false if a bounded wait gave up.
-template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
+template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN, int FOLD = 1>
 __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &args, int x0, int y0, int z0,
                                         const BPSmem<BPShape<TX, TY, ZT, A, S>> &sm, uint32_t &g)
 {
@@ -395,6 +395,12 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
     const int kMagicBits = __float_as_int(kMagic);
     const float eoff = axis - 1.0f + (PAIRS ? 1.0f : 0.0f);  // h - 0.5 - 0.5 (+1 for pairs)
     bool aborted = false;
+    // partial sums run over FOLD angle blocks before they are added (compensated) into the totals
+    float part[RY][ZT];
+#pragma unroll
+    for (int j = 0; j < RY; j++)
+#pragma unroll
+        for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
 
     for (int blk = 0; blk < nblk; blk++) {
         if (tid == 0 && blk + S - 1 < nblk) issue(blk + S - 1);
@@ -404,12 +410,6 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
         const int p0 = blk * A;
         const int nval = min(A, (int)P - p0);
         const uint32_t *sdata = data + (size_t)slot * A * ASTR;
-
-        float part[RY][ZT];
-#pragma unroll
-        for (int j = 0; j < RY; j++)
-#pragma unroll
-            for (int z = 0; z < ZT; z++) part[j][z] = 0.f;
 
         if (ok && PACK) {
             // single slice: the coordinate chain of two output rows runs as packed
@@ -500,19 +500,22 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
                 }
             }
         }
+        if ((blk + 1) % FOLD == 0 || blk + 1 == nblk) {
 #pragma unroll
-        for (int j = 0; j < RY; j++)
+            for (int j = 0; j < RY; j++)
 #pragma unroll
-            for (int z = 0; z < ZT; z++) {
-                if (KAHAN) {
-                    const float yk = part[j][z] - comp[j][z];
-                    const float tk = acc[j][z] + yk;
-                    comp[j][z] = (tk - acc[j][z]) - yk;
-                    acc[j][z] = tk;
-                } else {
-                    acc[j][z] += part[j][z];
+                for (int z = 0; z < ZT; z++) {
+                    if (KAHAN) {
+                        const float yk = part[j][z] - comp[j][z];
+                        const float tk = acc[j][z] + yk;
+                        comp[j][z] = (tk - acc[j][z]) - yk;
+                        acc[j][z] = tk;
+                    } else {
+                        acc[j][z] += part[j][z];
+                    }
+                    part[j][z] = 0.f;
                 }
-            }
+        }
         if (__syncthreads_or(!ok)) {
             aborted = true;
             break;
@@ -593,7 +596,7 @@ __global__ void __launch_bounds__(256) k_bp_batch(const BatchBP *__restrict__ jo
         const int tx = (int)(w.y % j->tiles_x), ty = (int)(w.y / j->tiles_x);
         if (threadIdx.x == 0)
             asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(&j->map) : "memory");
-        if (!bp_tile<TX, TY, 1, A, S, KIND, KAHAN>(&j->map, j->args, tx * TX, ty * TY, 0, sm, g)) break;
+        if (!bp_tile<TX, TY, 1, A, S, KIND, KAHAN, 2>(&j->map, j->args, tx * TX, ty * TY, 0, sm, g)) break;
     }
 }
 
