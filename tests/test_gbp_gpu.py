@@ -258,3 +258,38 @@ def test_compute_half_padded_rows_and_modes(cuda):
     t.set_property("compute-type", "float")
     full = t.process(torch.from_numpy(proj).cuda()).cpu().numpy()
     assert oracle.rel_l2(full, oracle_gbp(proj, props, addressing_mode="clamp_to_edge")) < 2e-5
+
+
+@pytest.mark.parametrize("store,tol", [("half", 3e-3), ("float", 2e-5), ("double", 2e-5)])
+def test_compute_half_with_store_types(cuda, store, tol):
+    """FP16 samples combine with every floating store type: equal (within the store's precision)
+    to the FP64 store semantics applied to FP16-rounded projections."""
+    props = dict(BASE, **GEOMETRIES["cone"])
+    proj = _proj(33, smooth=True)
+    rounded = proj.astype(np.float16).astype(np.float32)
+    got = run_gbp(proj, props, **{"compute-type": "half", "store-type": store}).cpu().numpy().astype(np.float64)
+    ref = oracle.general_backproject_store(rounded, N, store_type=store, region=(-4.0, 4.0, 1.0),
+                                           **{k: v for k, v in props.items() if k != "region"})
+    assert oracle.rel_l2(got, ref) < tol
+
+
+def test_compute_half_streaming_matches_one_shot(cuda):
+    """Projections passed one by one (process, then generate per slice) with FP16 samples give
+    the one-shot volume."""
+    props = dict(BASE, **GEOMETRIES["lamino"])
+    proj = _proj(34, smooth=True)
+    one = run_gbp(proj, props, **{"compute-type": "half"}).cpu().numpy()
+    t = ufob.GeneralBackprojectTask(num_projections=N)
+    for k, v in props.items():
+        t.set_property(k, v)
+    t.set_property("compute-type", "half")
+    L = ufob.lib()
+    dproj = torch.from_numpy(proj).cuda()
+    ow, oh, ns = t.get_requisition(W, H)
+    for i in range(N):
+        ufob.check(L.ufob_gbp_process(t._h, dproj[i].data_ptr(), W, H, None))
+    sl = torch.empty((oh, ow), dtype=torch.float32, device="cuda")
+    for z in range(ns):
+        ufob.check(L.ufob_gbp_generate(t._h, sl.data_ptr(), z, None))
+        torch.cuda.synchronize()
+        assert oracle.rel_l2(sl.cpu().numpy(), one[z]) < 1e-6
