@@ -347,6 +347,7 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
     const int nblk = (int)((P + A - 1) / A);
     const float axis = args.axis;
     const uint32_t g0 = g;
+    const float2 *sincos = args.sincos + (size_t)z0 * args.sincos_zstride;
 
     // Producer: stage block `blk` of this tile into slot (g0 + blk) % S.
     auto issue = [&](int blk) {
@@ -357,7 +358,7 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
         const float cx0 = (float)(args.roi_x + x0) - axis + 0.5f, cx1 = cx0 + (float)(TX - 1);
         const float cy0 = (float)(args.roi_y + y0) - axis + 0.5f, cy1 = cy0 + (float)(TY - 1);
         for (int a = 0; a < nval; a++) {
-            const float2 sc = args.sincos[p0 + a];
+            const float2 sc = sincos[p0 + a];
             float h0 = fmaf(cy0, sc.x, fmaf(cx0, sc.y, axis));
             float h1 = fmaf(cy0, sc.x, fmaf(cx1, sc.y, axis));
             float h2 = fmaf(cy1, sc.x, fmaf(cx0, sc.y, axis));
@@ -418,7 +419,7 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
             const uint64_t magic2 = f2pack(kMagic, kMagic), half2 = f2pack(0.5f, 0.5f);
 #pragma unroll 2
             for (int a = 0; a < nval; a++) {
-                const float2 sc = __ldg(&args.sincos[p0 + a]);
+                const float2 sc = __ldg(&sincos[p0 + a]);
                 const int xs = win[slot * A + a];
                 const float t = fmaf(bx, sc.y, eoff - (float)xs);
                 const uint64_t s2 = f2pack(sc.x, sc.x), t2 = f2pack(t, t);
@@ -455,7 +456,7 @@ __device__ __forceinline__ bool bp_tile(const CUtensorMap *map, const BPArgs &ar
         } else if (ok) {
 #pragma unroll 2
             for (int a = 0; a < nval; a++) {
-                const float2 sc = __ldg(&args.sincos[p0 + a]);
+                const float2 sc = __ldg(&sincos[p0 + a]);
                 const int xs = win[slot * A + a];
                 const float t = fmaf(bx, sc.y, eoff - (float)xs);
                 const uint32_t *row = sdata + a * ASTR;
@@ -958,7 +959,7 @@ ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t
 
 template <int TX, int TY, int ZT, int A, int S, int KIND, bool KAHAN>
 static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32_t elems, uint32_t pitch,
-                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream)
+                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream, uint32_t zstride = 0)
 {
     using Sh = BPShape<TX, TY, ZT, A, S>;
     auto kern = k_bp_linear<TX, TY, ZT, A, S, KIND, KAHAN>;
@@ -981,6 +982,7 @@ static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32
     a.sincos = g.d_sincos;
     a.out = d_out;
     a.err = device_error_word();
+    a.sincos_zstride = zstride;
     dim3 grid((g.roi_w + TX - 1) / TX, (g.roi_h + TY - 1) / TY, (g.nz + ZT - 1) / ZT);
     kern<<<grid, Sh::kThreads, Sh::kSmem, stream>>>(map, a);
     UFOB_CUDA_TRY(cudaGetLastError());
@@ -1197,5 +1199,51 @@ ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind k
                      : dispatch_tile<SINO_BF16_PAIRS, false>(tile, g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     }
 }
+
+// out[i] = sum over the angle groups of part[k][i], in group order
+__global__ void k_sum_groups(const float *__restrict__ part, uint64_t plane, uint32_t groups, float *__restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < plane; i += (uint64_t)gridDim.x * blockDim.x) {
+        float v = part[i];
+        for (uint32_t k = 1; k < groups; k++) v += part[(uint64_t)k * plane + i];
+        out[i] = v;
+    }
+}
+
+ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
+                                   uint32_t groups, float *d_part, float *d_out, bool kahan, cudaStream_t stream)
+{
+    if (!groups || g.nz != 1 || g.P % groups)
+        return fail(UFOB_ERR_INVALID, "backproject: %u angle groups for %u rows of one sinogram", groups, g.P);
+    if (((uintptr_t)d_sino & 15) || (pitch & 3))
+        return fail(UFOB_ERR_INVALID, "backproject: sinogram base/pitches must be 16-byte aligned");
+    BPGeometry gg = g;
+    gg.P = g.P / groups;  // rows per group; the norm stays pi / (all rows)
+    gg.nz = groups;
+    const uint32_t elems = kind == SINO_F32 ? g.W : g.W + 1;
+    const uint64_t sp = (uint64_t)gg.P * pitch;
+    ufob_status st;
+    if (kind == SINO_F32)
+        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_F32, true>(gg, d_sino, elems, pitch, sp, d_part, stream, gg.P)
+                   : launch_linear<32, 96, 1, 16, 3, SINO_F32, false>(gg, d_sino, elems, pitch, sp, d_part, stream, gg.P);
+    else if (kind == SINO_F16_PAIRS)
+        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_F16_PAIRS, true>(gg, d_sino, elems, pitch, sp, d_part, stream,
+                                                                           gg.P)
+                   : launch_linear<32, 96, 1, 16, 3, SINO_F16_PAIRS, false>(gg, d_sino, elems, pitch, sp, d_part, stream,
+                                                                            gg.P);
+    else
+        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_BF16_PAIRS, true>(gg, d_sino, elems, pitch, sp, d_part, stream,
+                                                                            gg.P)
+                   : launch_linear<32, 96, 1, 16, 3, SINO_BF16_PAIRS, false>(gg, d_sino, elems, pitch, sp, d_part,
+                                                                             stream, gg.P);
+    UFOB_TRY(st);
+    const uint64_t plane = (uint64_t)g.roi_w * g.roi_h;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((plane + 255) / 256, (uint64_t)num_sms() * 8);
+    k_sum_groups<<<grid, 256, 0, stream>>>(d_part, plane, groups, d_out);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
 
 }  // namespace ufob

@@ -371,6 +371,7 @@ struct ufob_backproject {
     ufob_bp_props props;
     DevBuf sincos;
     DevBuf aligned;  // copy of a sinogram whose pitch is not TMA-compatible
+    DevBuf partial;  // per-angle-group images of one small sinogram (split_groups)
     // cache key of the sin/cos table
     uint32_t key_P = 0, key_nproj = 0, key_offset = 0;
     double key_step = 0, key_aoff = 0;
@@ -526,6 +527,23 @@ static bool want_kahan(const ufob_bp_props &p, SinoKind kind, uint32_t P)
     return kind != SINO_F32 && P >= 1500;
 }
 
+// A single sinogram whose slice gives the SMs fewer than two 32x96 tiles each is split into
+// 2, 4 or 8 angle groups (equal, at least 32 angles each) whose partial images are summed, so
+// that the tall tile still fills the GPU; 1 = no split.
+static uint32_t split_groups(const BPGeometry &g)
+{
+    if (g.nz != 1) return 1;
+    const uint64_t tiles = (uint64_t)((g.roi_w + 31) / 32) * ((g.roi_h + 95) / 96), sms = (uint64_t)num_sms();
+    if (tiles >= 2 * sms) return 1;
+    uint32_t best = 1;
+    for (uint32_t k = 2; k <= 8; k *= 2) {
+        if (g.P % k || g.P / k < 32) break;
+        best = k;
+        if (tiles * k >= 2 * sms) break;
+    }
+    return tiles * best >= sms ? best : 1;
+}
+
 extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_dtype dtype,
                                             ufob_layout layout, uint32_t width, uint32_t height, uint32_t nslices,
                                             uint32_t pitch, uint64_t slice_pitch, float *d_out, void *stream)
@@ -576,8 +594,13 @@ extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_
         pitch = ap;
         slice_pitch = (uint64_t)ap * height;
     }
-    return bp_linear_launch(g, src, kind, pitch, slice_pitch, d_out, want_kahan(bp->props, kind, height),
-                            bp->props.tile, s);
+    const bool kahan = want_kahan(bp->props, kind, height);
+    const uint32_t groups = bp->props.tile < 0 ? split_groups(g) : 1;
+    if (groups > 1) {
+        UFOB_TRY(bp->partial.ensure((size_t)groups * g.roi_w * g.roi_h * sizeof(float)));
+        return bp_linear_split_launch(g, src, kind, pitch, groups, bp->partial.as<float>(), d_out, kahan, s);
+    }
+    return bp_linear_launch(g, src, kind, pitch, slice_pitch, d_out, kahan, bp->props.tile, s);
 }
 
 extern "C" void ufob_backproject_destroy(ufob_backproject *bp) { delete bp; }

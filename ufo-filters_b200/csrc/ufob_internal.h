@@ -225,6 +225,10 @@ enum SinoKind { SINO_F32 = 0, SINO_F16_PAIRS = 1, SINO_BF16_PAIRS = 2 };
 
 ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
                              uint64_t slice_pitch, float *d_out, bool kahan, int tile, cudaStream_t stream);
+// One sinogram split into `groups` angle groups of height / groups rows (tile 8, slice z = group
+// z), partial images summed into d_out; d_part holds groups x roi_h x roi_w floats.
+ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
+                                   uint32_t groups, float *d_part, float *d_out, bool kahan, cudaStream_t stream);
 
 // Slice-quad FP16 form (four slices' tap pairs per 16-byte cell): filter stage
 // and backprojection.  acc: 0 FP32 accumulation of every product, 1 FP16 lerp
@@ -244,6 +248,9 @@ struct BPArgs {
     const float2 *sincos;
     float *out;
     int *err;
+    // angle-table entries between consecutive slices: 0 for a stack (all slices share the
+    // angles); the group length when the slices are angle groups of one sinogram
+    uint32_t sincos_zstride = 0;
 };
 
 // ------------------------------------------------------- uneven batches (persistent kernels)
