@@ -527,21 +527,28 @@ static bool want_kahan(const ufob_bp_props &p, SinoKind kind, uint32_t P)
     return kind != SINO_F32 && P >= 1500;
 }
 
-// A single sinogram whose slice gives the SMs fewer than two 32x96 tiles each is split into
-// 2, 4 or 8 angle groups (equal, at least 32 angles each) whose partial images are summed, so
-// that the tall tile still fills the GPU; 1 = no split.
+// A single sinogram is split into 2, 4 or 8 equal angle groups (at least 32 angles each) whose
+// partial images are summed, when that spreads its 32x96 tiles more evenly over the SMs: the
+// busiest SM's share of tiles over the average one drops by more than 5%; 1 = no split.
 static uint32_t split_groups(const BPGeometry &g)
 {
     if (g.nz != 1) return 1;
-    const uint64_t tiles = (uint64_t)((g.roi_w + 31) / 32) * ((g.roi_h + 95) / 96), sms = (uint64_t)num_sms();
-    if (tiles >= 2 * sms) return 1;
+    const double tiles = (double)((g.roi_w + 31) / 32) * (double)((g.roi_h + 95) / 96), sms = (double)num_sms();
+    auto imbalance = [&](uint32_t k) {
+        const double per_sm = tiles * k / sms;
+        return std::ceil(per_sm) / per_sm;
+    };
     uint32_t best = 1;
+    double best_im = imbalance(1);
     for (uint32_t k = 2; k <= 8; k *= 2) {
         if (g.P % k || g.P / k < 32) break;
-        best = k;
-        if (tiles * k >= 2 * sms) break;
+        const double im = imbalance(k);
+        if (im < best_im - 0.05) {
+            best = k;
+            best_im = im;
+        }
     }
-    return tiles * best >= sms ? best : 1;
+    return best;
 }
 
 extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_sino, ufob_dtype dtype,
