@@ -1,11 +1,20 @@
 """The reference itself, run on the CPU (TEST INFRASTRUCTURE ONLY).
 
 ``_ref/libufo_ref.so`` (built by ``make -f ref.mk`` from the reference sources)
-holds the reference's own ``filter`` and ``backproject`` task code
-(src/ufo-filter-task.c, src/ufo-backproject-task.c) and its OpenCL kernels
+holds the reference's own ``filter``, ``backproject`` and ``general-backproject``
+task code (src/ufo-filter-task.c, src/ufo-backproject-task.c,
+src/ufo-general-backproject-task.c with src/common/ufo-scarray.c,
+ufo-ctgeometry.c, ufo-conebeam.c) and its OpenCL kernels
 (src/kernels/backproject.cl, filter.cl, fft.cl, forwardproject.cl, ffc.cl,
 conebeam.cl) compiled for the CPU against small GLib/OpenCL/ufo-core shims.  The FFT library the
-reference calls (vendored oclfft or clFFT) is replaced by an FP64 FFT.
+reference calls (vendored oclfft or clFFT) is replaced by an FP64 FFT.  The
+kernels ``general-backproject`` generates at run time from
+src/kernels/templates/general_bp_*.in, and the ``lamino-backproject`` kernels
+its build writes with src/kernels/tools/make_burst_kernels.py (run here the way
+src/kernels/meson.build:59-83 runs it), are compiled for the CPU when the tasks
+ask for them (refshim/ref_clc_jit.cpp), which needs the reference tree
+(``UFO_FILTERS_SOURCE``) and g++.  ``lamino-backproject`` (src/ufo-lamino-
+backproject-task.c, src/lamino-roi.c) is in the library too.
 
 Used to pin the FP64 oracle (oracle.py) and to generate the golden fixtures
 under tests/golden/, and as the reference arm of the CPU baseline.
@@ -20,6 +29,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libufo_ref.so")
+REF_SOURCE = os.environ.get("UFO_FILTERS_SOURCE", "/root/reference")
 _LIB = None
 
 FILTERS = ["ramp", "ramp-fromreal", "butterworth", "faris-byer", "hamming", "bh3"]
@@ -53,6 +63,20 @@ def lib():
         L.ref_forwardproject.argtypes = [vp, i, i, f, f, vp]
         L.ref_flat_correct.argtypes = [vp, vp, vp, vp, i, i, i, i, i, f, f]
         L.ref_weight_projection.argtypes = [vp, vp, i, i, f, f, f, f, f, f]
+        L.ref_gbp_new.restype = vp
+        L.ref_gbp_set.argtypes = [vp, ctypes.c_char_p, vp, u, ctypes.c_char_p]
+        L.ref_gbp_set.restype = i
+        L.ref_gbp_run.argtypes = [vp, vp, u, u, u, vp, ctypes.c_size_t, ctypes.POINTER(u), ctypes.c_char_p, i]
+        L.ref_gbp_run.restype = i
+        L.ref_lamino_new.restype = vp
+        L.ref_lamino_set.argtypes = [vp, ctypes.c_char_p, vp, u, ctypes.c_char_p]
+        L.ref_lamino_set.restype = i
+        L.ref_lamino_run.argtypes = [vp, vp, u, u, u, vp, ctypes.c_size_t, ctypes.POINTER(u), ctypes.c_char_p, i]
+        L.ref_lamino_run.restype = i
+        L.refshim_set_dirs.argtypes = [ctypes.c_char_p] * 3
+        L.refshim_set_device_limits.argtypes = [ctypes.c_ulong] * 3
+        L.refshim_set_dirs(os.path.join(REF_SOURCE, "src", "kernels", "templates").encode(),
+                           os.path.join(HERE, "refshim").encode(), os.path.join(HERE, "_ref", "jit").encode())
         _LIB = L
     return _LIB
 
@@ -154,4 +178,116 @@ def weight_projection(proj, cx, cz, sd, od, mr, cs):
     out = np.empty_like(proj)
     lib().ref_weight_projection(_p(proj), _p(out), W, H, float(cx), float(cz), float(sd), float(od), float(mr),
                                 float(cs))
+    return out
+
+
+GBP_ENUMS = ("parameter", "compute-type", "result-type", "store-type", "addressing-mode")
+GBP_STORE_DTYPES = {"half": np.float16, "float": np.float32, "double": np.float64, "uchar": np.uint8,
+                    "ushort": np.uint16, "uint": np.uint32}
+
+
+def general_backproject(proj, props, max_alloc_slices=0):
+    """The reference's ``general-backproject`` task over projections ``proj``
+    [n, height, width] with ``props`` = {reference property name: value}
+    (scalars, sequences for the array properties, value nicks for the
+    enumerations).  The task generates its OpenCL kernel (make_kernel), which
+    runs on the CPU with the exact-weight linear sampler.  ``max_alloc_slices``
+    > 0 reports a device allocation limit of that many slices so that the task
+    splits its volume into chunks.  Returns the volume [slices, y, x] in the
+    store type."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    n, h, w = proj.shape
+    L = lib()
+    t = L.ref_gbp_new()
+    props = dict(props)
+    props.setdefault("num-projections", n)
+    store = props.get("store-type", "float")
+    for name, value in props.items():
+        if name in GBP_ENUMS:
+            rc = L.ref_gbp_set(t, name.encode(), None, 0, str(value).encode())
+        else:
+            arr = np.atleast_1d(np.asarray(value, dtype=np.float64))
+            rc = L.ref_gbp_set(t, name.encode(), _p(arr), arr.size, None)
+        if rc:
+            raise ValueError("general-backproject: unknown property or value %s=%r" % (name, value))
+    dims = (ctypes.c_uint * 4)()
+    err = ctypes.create_string_buffer(512)
+    # first pass: requisition only (volume dimensions)
+    probe = L.ref_gbp_new()
+    for name, value in props.items():
+        if name in GBP_ENUMS:
+            L.ref_gbp_set(probe, name.encode(), None, 0, str(value).encode())
+        else:
+            arr = np.atleast_1d(np.asarray(value, dtype=np.float64))
+            L.ref_gbp_set(probe, name.encode(), _p(arr), arr.size, None)
+    rc = L.ref_gbp_run(probe, _p(proj), w, h, min(n, 1), None, 0, dims, err, 512)
+    if rc < 0:
+        raise ValueError(err.value.decode())
+    nx, ny, nz, bpp = dims[0], dims[1], dims[2], dims[3]
+    slice_bytes = nx * ny * bpp
+    L.refshim_set_device_limits(64 << 30, slice_bytes * max_alloc_slices if max_alloc_slices else 4 << 30, 256)
+    try:
+        out = np.zeros((nz, ny, nx), dtype=GBP_STORE_DTYPES[store])
+        rc = L.ref_gbp_run(t, _p(proj), w, h, n, _p(out), out.nbytes, dims, err, 512)
+    finally:
+        L.refshim_set_device_limits(64 << 30, 4 << 30, 256)
+    if rc < 0:
+        raise ValueError(err.value.decode())
+    return out
+
+
+LAMINO_KERNELS = ("z", "lamino", "center", "roll")
+LAMINO_ENUMS = ("parameter", "addressing-mode")
+
+
+def _lamino_kernel_files():
+    """Write {z,lamino,center,roll}_kernel.cl with the reference's generator, with the bursts
+    its build passes (src/kernels/meson.build:66-70)."""
+    jit = os.path.join(HERE, "_ref", "jit")
+    os.makedirs(jit, exist_ok=True)
+    tools = os.path.join(REF_SOURCE, "src", "kernels", "tools", "make_burst_kernels.py")
+    for name in LAMINO_KERNELS:
+        path = os.path.join(jit, name + "_kernel.cl")
+        if not os.path.exists(path):
+            tmpl = os.path.join(REF_SOURCE, "src", "kernels", "templates", name + "_template.in")
+            src = subprocess.check_output(["python3", tools, tmpl, "1", "2", "4", "8", "16"], text=True)
+            with open(path + ".tmp", "w") as f:
+                f.write(src)
+            os.replace(path + ".tmp", path)
+
+
+def lamino_backproject(proj, props):
+    """The reference's ``lamino-backproject`` task over projections [n, height, width] with
+    ``props`` = {reference property name: value}; returns the FP32 volume [z, y, x]."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    n, h, w = proj.shape
+    _lamino_kernel_files()
+    L = lib()
+    t = L.ref_lamino_new()
+    props = dict(props)
+    props.setdefault("num-projections", n)
+    for name, value in props.items():
+        if name in LAMINO_ENUMS:
+            rc = L.ref_lamino_set(t, name.encode(), None, 0, str(value).encode())
+        else:
+            arr = np.atleast_1d(np.asarray(value, dtype=np.float64))
+            rc = L.ref_lamino_set(t, name.encode(), _p(arr), arr.size, None)
+        if rc:
+            raise ValueError("lamino-backproject: unknown property or value %s=%r" % (name, value))
+    dims = (ctypes.c_uint * 4)()
+    err = ctypes.create_string_buffer(512)
+    rc = L.ref_lamino_run(t, _p(proj), w, h, 0, None, 0, dims, err, 512)
+    if rc < 0:
+        raise ValueError(err.value.decode())
+    out = np.zeros((dims[2], dims[1], dims[0]), dtype=np.float32)
+    t = L.ref_lamino_new()
+    for name, value in props.items():
+        if name in LAMINO_ENUMS:
+            L.ref_lamino_set(t, name.encode(), None, 0, str(value).encode())
+        else:
+            arr = np.atleast_1d(np.asarray(value, dtype=np.float64))
+            L.ref_lamino_set(t, name.encode(), _p(arr), arr.size, None)
+    rc = L.ref_lamino_run(t, _p(proj), w, h, n, _p(out), out.size, dims, err, 512)
+    if rc < 0:
+        raise ValueError(err.value.decode())
     return out

@@ -19,6 +19,9 @@
 #define __write_only
 typedef unsigned int uint;
 #define M_PI_F 3.14159265358979323846f
+extern thread_local size_t clshim_gid[3], clshim_gsz[3];
+inline size_t get_global_id(int d) { return clshim_gid[d]; }
+inline size_t get_global_size(int d) { return clshim_gsz[d]; }
 inline float sincos(float x, float *c)
 {
     *c = std::cos(x);

@@ -1,4 +1,5 @@
-// Types of the OpenCL C kernel-language shim (see clc_shim.hpp).  Test infrastructure only.
+// Types of the OpenCL C kernel-language shim (see clc_shim.hpp, clc_gen.hpp).
+// Test infrastructure only.
 #pragma once
 #include <cmath>
 #include <cstddef>
@@ -27,16 +28,39 @@ typedef int sampler_t;
 #define CLK_FILTER_NEAREST 0x10
 #define CLK_FILTER_LINEAR 0x20
 
+// A single-channel FP32 image (CL_INTENSITY / CL_R with CL_FLOAT).
 struct image2d_t {
     const float *data;
     int width, height;
 };
 
-// Linear/nearest sampling with unnormalised coordinates: texel (i, j) is
-// centred at (i + 0.5, j + 0.5); CLK_ADDRESS_CLAMP returns the border value 0
-// outside the image, CLK_ADDRESS_CLAMP_TO_EDGE (and NONE) clamp the index.
-float4 read_imagef(image2d_t img, sampler_t s, float2 coord);
+inline float clshim_texel(const image2d_t &img, int i, int j, int addr)
+{
+    if (i < 0 || j < 0 || i >= img.width || j >= img.height) {
+        if (addr == CLK_ADDRESS_CLAMP) return 0.f;
+        i = i < 0 ? 0 : (i >= img.width ? img.width - 1 : i);
+        j = j < 0 ? 0 : (j >= img.height ? img.height - 1 : j);
+    }
+    return img.data[(size_t)j * img.width + i];
+}
 
-extern thread_local size_t clshim_gid[3], clshim_gsz[3];
-inline size_t get_global_id(int d) { return clshim_gid[d]; }
-inline size_t get_global_size(int d) { return clshim_gsz[d]; }
+// Linear/nearest sampling with unnormalised coordinates: texel (i, j) is
+// centred at (i + 0.5, j + 0.5) and the linear weights are exact (the CPU
+// OpenCL semantics); CLK_ADDRESS_CLAMP returns the border value 0 outside the
+// image, CLK_ADDRESS_CLAMP_TO_EDGE (and NONE) clamp the index.
+inline float4 read_imagef(image2d_t img, sampler_t s, float2 c)
+{
+    const int addr = s & 0xe;
+    float v;
+    if (s & CLK_FILTER_LINEAR) {
+        const float u = c.x - 0.5f, w = c.y - 0.5f;
+        const float fu = std::floor(u), fw = std::floor(w);
+        const float a = u - fu, b = w - fw;
+        const int i = (int)fu, j = (int)fw;
+        v = (1.f - a) * (1.f - b) * clshim_texel(img, i, j, addr) + a * (1.f - b) * clshim_texel(img, i + 1, j, addr) +
+            (1.f - a) * b * clshim_texel(img, i, j + 1, addr) + a * b * clshim_texel(img, i + 1, j + 1, addr);
+    } else {
+        v = clshim_texel(img, (int)std::floor(c.x), (int)std::floor(c.y), addr);
+    }
+    return float4{v, 0.f, 0.f, 1.f};
+}

@@ -1,0 +1,2 @@
+/* GLib printf family of the shim (see glib.h).  Test infrastructure only. */
+#include <glib.h>

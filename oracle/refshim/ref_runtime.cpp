@@ -19,35 +19,6 @@ extern "C" {
 
 thread_local size_t clshim_gid[3], clshim_gsz[3];
 
-// ------------------------------------------------------------------ sampler
-
-static inline float texel(const image2d_t &img, int i, int j, int addr)
-{
-    if (i < 0 || j < 0 || i >= img.width || j >= img.height) {
-        if (addr == CLK_ADDRESS_CLAMP) return 0.f;
-        i = i < 0 ? 0 : (i >= img.width ? img.width - 1 : i);
-        j = j < 0 ? 0 : (j >= img.height ? img.height - 1 : j);
-    }
-    return img.data[(size_t)j * img.width + i];
-}
-
-float4 read_imagef(image2d_t img, sampler_t s, float2 c)
-{
-    const int addr = s & 0xe;
-    float v;
-    if (s & CLK_FILTER_LINEAR) {
-        const float u = c.x - 0.5f, w = c.y - 0.5f;
-        const float fu = floorf(u), fw = floorf(w);
-        const float a = u - fu, b = w - fw;
-        const int i = (int)fu, j = (int)fw;
-        v = (1.f - a) * (1.f - b) * texel(img, i, j, addr) + a * (1.f - b) * texel(img, i + 1, j, addr) +
-            (1.f - a) * b * texel(img, i, j + 1, addr) + a * b * texel(img, i + 1, j + 1, addr);
-    } else {
-        v = texel(img, (int)floorf(c.x), (int)floorf(c.y), addr);
-    }
-    return float4{v, 0.f, 0.f, 1.f};
-}
-
 // ------------------------------------------------------------------ kernels compiled from the reference
 extern "C" {
 void backproject_tex(image2d_t, float *, const float *, const float *, unsigned, unsigned, unsigned, unsigned, float);
@@ -89,7 +60,9 @@ template <typename F> static void ndrange(guint ndims, const gsize *g, F body)
 extern "C" void refshim_dispatch(refshim_kernel *k, guint ndims, const gsize *g)
 {
     const char *n = k->name;
-    if (!strcmp(n, "backproject_tex")) {
+    if (k->jit) {
+        refshim_jit_dispatch(k, ndims, g, NULL);
+    } else if (!strcmp(n, "backproject_tex")) {
         image2d_t img = img_arg(k, 0);
         float *out = mem_ptr(k, 1);
         const float *s = mem_ptr(k, 2), *c = mem_ptr(k, 3);
@@ -250,8 +223,10 @@ UfoProfiler *ufo_task_node_get_profiler(UfoTaskNode *) { return NULL; }
 cl_command_queue ufo_gpu_node_get_cmd_queue(UfoGpuNode *) { return NULL; }
 cl_context ufo_resources_get_context(UfoResources *) { return NULL; }
 
-cl_kernel ufo_resources_get_kernel(UfoResources *, const char *, const char *name, const char *, GError **)
+cl_kernel ufo_resources_get_kernel(UfoResources *, const char *file, const char *name, const char *, GError **err)
 {
+    const size_t fl = file ? strlen(file) : 0;
+    if (fl > 10 && !strcmp(file + fl - 10, "_kernel.cl")) return refshim_jit_from_file(file, name, err);
     cl_kernel k = (cl_kernel)calloc(1, sizeof(refshim_kernel));
     snprintf(k->name, sizeof k->name, "%s", name);
     return k;
@@ -259,14 +234,18 @@ cl_kernel ufo_resources_get_kernel(UfoResources *, const char *, const char *nam
 
 void refshim_buffer_init(UfoBuffer *b, float *data, guint n_dims, gsize d0, gsize d1, gsize d2)
 {
+    refshim_buffer_init_bytes(b, data, d0 * d1 * d2 * sizeof(float), n_dims, d0, d1, d2);
+}
+void refshim_buffer_init_bytes(UfoBuffer *b, void *data, size_t bytes, guint n_dims, gsize d0, gsize d1, gsize d2)
+{
     memset(b, 0, sizeof *b);
     b->req.n_dims = n_dims;
     b->req.dims[0] = d0;
     b->req.dims[1] = d1;
     b->req.dims[2] = d2;
-    b->data = data;
+    b->data = (float *)data;
     b->mem.host = data;
-    b->mem.size = d0 * d1 * d2 * sizeof(float);
+    b->mem.size = bytes;
 }
 
 void ufo_buffer_get_requisition(UfoBuffer *b, UfoRequisition *r) { *r = b->req; }
@@ -282,9 +261,18 @@ cl_mem ufo_buffer_get_device_image(UfoBuffer *b, cl_command_queue)
     b->mem.height = (int)b->req.dims[1];
     return &b->mem;
 }
-void ufo_profiler_call(UfoProfiler *, cl_command_queue, cl_kernel k, guint ndims, const gsize *global, const gsize *)
+void ufo_profiler_call(UfoProfiler *, cl_command_queue, cl_kernel k, guint ndims, const gsize *global,
+                       const gsize *local)
 {
-    refshim_dispatch(k, ndims, global);
+    if (k->jit)
+        refshim_jit_dispatch(k, ndims, global, local);
+    else
+        refshim_dispatch(k, ndims, global);
+}
+void ufo_profiler_call_blocking(UfoProfiler *p, cl_command_queue q, cl_kernel k, guint ndims, const gsize *global,
+                                const gsize *local)
+{
+    ufo_profiler_call(p, q, k, ndims, global, local);
 }
 
 // The two element-wise kernels of the fft / ifft tasks, launched with the

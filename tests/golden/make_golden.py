@@ -1,12 +1,14 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-The reference's `filter` and `backproject` task sources and its OpenCL kernels
-(with the flat-field and cone-beam weight kernels) are compiled for the CPU by oracle/ref.mk (oracle/_ref/libufo_ref.so, see
-oracle/reference.py); this script runs them on seeded inputs and stores inputs
-and outputs.  Run it where the reference sources are present:
+The reference's `filter`, `backproject` and `general-backproject` task sources and its OpenCL
+kernels (with the flat-field and cone-beam weight kernels) are compiled for the CPU by oracle/ref.mk
+(oracle/_ref/libufo_ref.so, see oracle/reference.py); the kernels general-backproject generates at
+run time are compiled when the task asks for them.  This script runs them on seeded inputs and
+stores inputs and outputs.  Run it where the reference sources are present:
 
-    make -C oracle -f ref.mk && python tests/golden/make_golden.py
+    make -C oracle -f ref.mk && python tests/golden/make_golden.py [fbp|pre|gbp ...]
 """
+import json
 import math
 import os
 import sys
@@ -15,6 +17,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+sys.path.insert(0, os.path.join(HERE, ".."))
+import gbp_cases  # noqa: E402
 import oracle  # noqa: E402  (phantom generators only)
 import reference  # noqa: E402
 
@@ -56,7 +60,6 @@ def main():
     path = os.path.join(HERE, "reference_fbp.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")
-    pre_golden()
 
 
 FFC_CASES = [dict(), dict(absorption_correct=True), dict(absorption_correct=True, fix_nan_and_inf=True),
@@ -88,5 +91,26 @@ def pre_golden():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def gbp_golden():
+    """The reference's general-backproject task on the cases of tests/gbp_cases.py."""
+    inputs = gbp_cases.make_inputs()
+    out = {"in_" + k: (v.astype(np.float16) if k == "d" else v) for k, v in inputs.items()}
+    out["cases"] = np.array(json.dumps(gbp_cases.CASES))
+    for c in gbp_cases.CASES:
+        vol = reference.general_backproject(inputs[c["input"]], c["props"],
+                                            max_alloc_slices=c.get("max_alloc_slices", 0))
+        out["out_" + c["name"]] = vol
+        print("  %-28s %s %s" % (c["name"], vol.shape, vol.dtype))
+    path = os.path.join(HERE, "reference_gbp.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1:] or ["fbp", "pre", "gbp"]
+    if "fbp" in which:
+        main()
+    if "pre" in which:
+        pre_golden()
+    if "gbp" in which:
+        gbp_golden()
