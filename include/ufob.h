@@ -180,8 +180,9 @@ void ufob_backproject_destroy(ufob_backproject *bp);
  * the reference).  For callers that cannot allocate device memory: hosts that
  * manage every byte of device memory in their own pool, and acquisition
  * pipelines that must not risk the device-wide synchronisation an allocation
- * can imply.  Same result as
- * ufob_backproject_run() with the same properties, but stateless and without
+ * can imply.  Same result as ufob_backproject_run() with the same properties
+ * within round-off (a single sinogram is not split into angle groups here, so
+ * its partial sums are added in another order), but stateless and without
  * any cudaMalloc/cudaFree: the only scratch, the per-angle sin/cos table,
  * lives in a fixed device array of UFOB_STATIC_MAX_ANGLES entries (256 KiB,
  * held by every GPU that loads the library until the process exits).
@@ -496,6 +497,9 @@ ufob_status ufob_conv3x3_wgrad(const void *d_in, const void *d_dz, float *d_dw, 
                                int cout, void *stream);
 /* Number of engine kernels launched by this process so far. */
 uint64_t ufob_launch_count(void);
+/* Number of device allocations (cudaMalloc) the engine has made in this
+ * process so far; its workspaces grow on demand and are reused. */
+uint64_t ufob_device_alloc_count(void);
 /* Sustained shared-memory load bandwidth (GB/s, 32-bit conflict-free loads)
  * and FP32 FMA throughput (TFLOP/s) of the current device, measured by two
  * short micro-kernels: the on-chip ceilings of voxel-driven backprojection. */

@@ -1,5 +1,5 @@
 # Builds oracle/_ref/libufo_ref.so: the reference's own task sources (filter,
-# backproject, general-backproject, lamino-backproject, with the common/
+# backproject, general-backproject, lamino-backproject, stacked-backproject, with the common/
 # helpers they use)
 # and OpenCL kernels (plus the flat-field and cone-beam weight kernels) compiled
 # for the CPU from where they lie under the reference tree, against the shims
@@ -51,12 +51,16 @@ $(OUT)/gbp_task.o: refshim/ref_gbp_task.c refshim/refshim_internal.h refshim/gli
 	@mkdir -p $(OUT)
 	$(CC) $(CFLAGS) -c $< -o $@
 
+$(OUT)/stacked_task.o: refshim/ref_stacked_task.c refshim/refshim_internal.h refshim/glib.h $(REF)/src/ufo-stacked-backproject-task.c
+	@mkdir -p $(OUT)
+	$(CC) $(CFLAGS) -c $< -o $@
+
 $(OUT)/lamino_task.o: refshim/ref_lamino_task.c refshim/refshim_internal.h refshim/glib.h $(REF)/src/ufo-lamino-backproject-task.c
 	@mkdir -p $(OUT)
 	$(CC) $(CFLAGS) -c $< -o $@
 
 OBJS := $(OUT)/kernels.o $(OUT)/kernels_pre.o $(OUT)/ref_runtime.o $(OUT)/ref_glib.o $(OUT)/ref_clc_jit.o \
-	$(OUT)/filter_task.o $(OUT)/backproject_task.o $(OUT)/gbp_task.o $(OUT)/lamino_task.o \
+	$(OUT)/filter_task.o $(OUT)/backproject_task.o $(OUT)/gbp_task.o $(OUT)/lamino_task.o $(OUT)/stacked_task.o \
 	$(COMMON:%=$(OUT)/common_%.o)
 
 $(OUT)/libufo_ref.so: $(OBJS)

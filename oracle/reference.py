@@ -14,7 +14,9 @@ its build writes with src/kernels/tools/make_burst_kernels.py (run here the way
 src/kernels/meson.build:59-83 runs it), are compiled for the CPU when the tasks
 ask for them (refshim/ref_clc_jit.cpp), which needs the reference tree
 (``UFO_FILTERS_SOURCE``) and g++.  ``lamino-backproject`` (src/ufo-lamino-
-backproject-task.c, src/lamino-roi.c) is in the library too.
+backproject-task.c, src/lamino-roi.c) and ``stacked-backproject``
+(src/ufo-stacked-backproject-task.c; src/kernels/stacked-backproject.cl, whose
+work-groups run as OpenMP teams) are in the library too.
 
 Used to pin the FP64 oracle (oracle.py) and to generate the golden fixtures
 under tests/golden/, and as the reference arm of the CPU baseline.
@@ -73,9 +75,14 @@ def lib():
         L.ref_lamino_set.restype = i
         L.ref_lamino_run.argtypes = [vp, vp, u, u, u, vp, ctypes.c_size_t, ctypes.POINTER(u), ctypes.c_char_p, i]
         L.ref_lamino_run.restype = i
+        L.ref_stacked_new.restype = vp
+        L.ref_stacked_set.argtypes = [vp, ctypes.c_char_p, d, ctypes.c_char_p]
+        L.ref_stacked_set.restype = i
+        L.ref_stacked_run.argtypes = [vp, vp, u, u, u, vp, ctypes.c_size_t, ctypes.POINTER(u), ctypes.c_char_p, i]
+        L.ref_stacked_run.restype = i
         L.refshim_set_dirs.argtypes = [ctypes.c_char_p] * 3
         L.refshim_set_device_limits.argtypes = [ctypes.c_ulong] * 3
-        L.refshim_set_dirs(os.path.join(REF_SOURCE, "src", "kernels", "templates").encode(),
+        L.refshim_set_dirs(os.path.join(REF_SOURCE, "src", "kernels").encode(),
                            os.path.join(HERE, "refshim").encode(), os.path.join(HERE, "_ref", "jit").encode())
         _LIB = L
     return _LIB
@@ -289,5 +296,35 @@ def lamino_backproject(proj, props):
             L.ref_lamino_set(t, name.encode(), _p(arr), arr.size, None)
     rc = L.ref_lamino_run(t, _p(proj), w, h, n, _p(out), out.size, dims, err, 512)
     if rc < 0:
+        raise ValueError(err.value.decode())
+    return out
+
+
+def stacked_backproject(sino, props):
+    """The reference's ``stacked-backproject`` task on a stack [z, projections, width] with
+    ``props`` = {reference property name: value} ("precision-mode" by nick); returns the FP32
+    volume [z, roi height, roi width] (slices past the last full group of 2 or 4, which the task
+    leaves unwritten, stay zero)."""
+    sino = np.ascontiguousarray(sino, dtype=np.float32)
+    z, rows, w = sino.shape
+    L = lib()
+
+    def task():
+        t = L.ref_stacked_new()
+        for name, value in props.items():
+            if name == "precision-mode":
+                rc = L.ref_stacked_set(t, name.encode(), 0.0, str(value).encode())
+            else:
+                rc = L.ref_stacked_set(t, name.encode(), float(value), None)
+            if rc:
+                raise ValueError("stacked-backproject: unknown property or value %s=%r" % (name, value))
+        return t
+
+    dims = (ctypes.c_uint * 4)()
+    err = ctypes.create_string_buffer(512)
+    if L.ref_stacked_run(task(), _p(sino), w, rows, z, None, 0, dims, err, 512) < 0:
+        raise ValueError(err.value.decode())
+    out = np.zeros((dims[2], dims[1], dims[0]), dtype=np.float32)
+    if L.ref_stacked_run(task(), _p(sino), w, rows, z, _p(out), out.size, dims, err, 512) < 0:
         raise ValueError(err.value.decode())
     return out

@@ -15,6 +15,7 @@ inline float2 operator*(float2 a, float s) { return {s * a.x, s * a.y}; }
 inline float2 &operator+=(float2 &a, float2 b) { a.x += b.x; a.y += b.y; return a; }
 struct float4 {
     float x, y, z, w;
+    float2 xy() const { return {x, y}; }
 };
 typedef int sampler_t;
 // OpenCL 1.2 sampler bits
@@ -32,6 +33,13 @@ typedef int sampler_t;
 struct image2d_t {
     const float *data;
     int width, height;
+};
+
+// A 2-D image array with 1, 2 or 4 channels per texel of FP32, FP16 or
+// unsigned 8-bit values (type 0, 1, 2), layers stacked after each other.
+struct image2d_array_t {
+    void *data;
+    int width, height, layers, channels, type;
 };
 
 inline float clshim_texel(const image2d_t &img, int i, int j, int addr)

@@ -82,10 +82,17 @@ bool parse_signature(const std::string &src, const std::string &name, std::vecto
     return true;
 }
 
+bool uses_barriers(const std::string &src) { return src.find("barrier") != std::string::npos; }
+
 std::string rewrite(const std::string &src)
 {
     std::string s = std::regex_replace(src, std::regex("\\((float|double|int|uint)([2348])\\)\\s*\\("), "make_$1$2(");
-    s = std::regex_replace(s, std::regex("\\.xz\\b"), ".xz()");
+    s = std::regex_replace(s, std::regex("\\.(xz|xy)\\b"), ".$1()");
+    if (uses_barriers(s)) {
+        // work-group kernels: __local arrays shared by the team, barrier() = the team's barrier
+        s = std::regex_replace(s, std::regex("\\b(__local|local)\\b"), "static");
+        s = std::regex_replace(s, std::regex("\\bbarrier\\s*\\([^)]*\\)"), "clgen_barrier()");
+    }
     s = std::regex_replace(s, std::regex("(\\w+)\\.s([0-9a-f])\\b"), "clgen_elem($1, 0x$2)");
     s = std::regex_replace(s, std::regex("#pragma OPENCL[^\\n]*"), "");
     return s;
@@ -94,6 +101,7 @@ std::string rewrite(const std::string &src)
 struct Compiled {
     void *handle = nullptr;
     void (*run)(void **, const size_t *, const size_t *) = nullptr;
+    void (*run_groups)(void **, const size_t *, const size_t *) = nullptr; /* kernels with barriers */
 };
 std::map<std::string, Compiled> g_cache;
 std::mutex g_mutex;
@@ -155,16 +163,30 @@ GValue *ufo_gpu_node_get_info(UfoGpuNode *, UfoGpuNodeInfo info)
     return v;
 }
 
+// A kernel file of the reference (src/kernels, src/kernels/templates) or one
+// written before the run into the cache folder (the generated lamino kernels).
+static bool read_kernel_file(const std::string &filename, std::string &out)
+{
+    for (const std::string &dir : {g_kernels_dir, g_kernels_dir + "/templates", g_cache_dir}) {
+        std::ifstream f(dir + "/" + filename);
+        if (f) {
+            std::stringstream ss;
+            ss << f.rdbuf();
+            out = ss.str();
+            return true;
+        }
+    }
+    return false;
+}
+
 gchar *ufo_resources_get_kernel_source(UfoResources *, const gchar *filename, GError **err)
 {
-    std::ifstream f(g_kernels_dir + "/" + filename);
-    if (!f) {
+    std::string src;
+    if (!read_kernel_file(filename, src)) {
         g_set_error(err, 0, 0, "kernel source %s not found under %s", filename, g_kernels_dir.c_str());
         return NULL;
     }
-    std::stringstream ss;
-    ss << f.rdbuf();
-    return g_strdup(ss.str().c_str());
+    return g_strdup(src.c_str());
 }
 
 cl_kernel ufo_resources_get_kernel_from_source(UfoResources *, const gchar *source, const gchar *name, const gchar *,
@@ -176,23 +198,26 @@ cl_kernel ufo_resources_get_kernel_from_source(UfoResources *, const gchar *sour
         g_set_error(err, 0, 0, "kernel %s: signature not understood", name);
         return NULL;
     }
-    std::ostringstream w;
-    w << "#include \"clc_gen.hpp\"\n" << body
-      << "\n\nextern \"C\" __attribute__((visibility(\"default\"))) void refshim_gen_run(void **a, const size_t *g, "
-      << "const size_t *l)\n{\n    (void)l;\n    CLGEN_NDRANGE(g, " << name << "(";
+    std::ostringstream call, w;
+    call << name << "(";
     for (size_t i = 0; i < params.size(); i++) {
         const Param &p = params[i];
-        if (i) w << ", ";
+        if (i) call << ", ";
         if (p.kind == 'p')
-            w << "(" << p.type << " *)a[" << i << "]";
-        else if (p.kind == 'i')
-            w << "*(image2d_t *)a[" << i << "]";
+            call << "(" << p.type << " *)a[" << i << "]";
         else if (p.kind == 's')
-            w << "*(sampler_t *)a[" << i << "]";
+            call << "*(sampler_t *)a[" << i << "]";
         else
-            w << "*(" << p.type << " *)a[" << i << "]";
+            call << "*(" << p.type << " *)a[" << i << "]";
     }
-    w << "));\n}\n";
+    call << ")";
+    const bool groups = uses_barriers(body);
+    w << "#include \"clc_gen.hpp\"\n" << body
+      << "\n\nextern \"C\" __attribute__((visibility(\"default\"))) void refshim_gen_run(void **a, const size_t *g, "
+      << "const size_t *l)\n{\n    (void)l;\n    CLGEN_NDRANGE(g, " << call.str() << ");\n}\n";
+    if (groups)
+        w << "extern \"C\" __attribute__((visibility(\"default\"))) void refshim_gen_run_groups(void **a, "
+          << "const size_t *g, const size_t *l)\n{\n    CLGEN_WORKGROUPS(g, l, " << call.str() << ");\n}\n";
     const std::string code = w.str();
     const std::string key = std::to_string(std::hash<std::string>()(code));
 
@@ -204,7 +229,7 @@ cl_kernel ufo_resources_get_kernel_from_source(UfoResources *, const gchar *sour
         if (!file_exists(so)) {
             std::ofstream(base + ".cpp") << code;
             const std::string tmp = base + "." + std::to_string(getpid()) + ".so";
-            const std::string cmd = "g++ -O2 -std=c++17 -fPIC -shared -fopenmp -w -Wno-psabi -mfma -ffp-contract=fast "
+            const std::string cmd = "g++ -O2 -std=c++17 -fPIC -shared -fopenmp -w -Wno-psabi -Wno-narrowing -mfma -ffp-contract=fast "
                                     "-fvisibility=hidden -I'" + g_shim_dir + "' -o '" + tmp + "' '" + base +
                                     ".cpp' > '" + base + ".log' 2>&1 && mv -f '" + tmp + "' '" + so + "'";
             if (system(cmd.c_str()) != 0) {
@@ -219,6 +244,7 @@ cl_kernel ufo_resources_get_kernel_from_source(UfoResources *, const gchar *sour
             return NULL;
         }
         c.run = (void (*)(void **, const size_t *, const size_t *))dlsym(c.handle, "refshim_gen_run");
+        c.run_groups = (void (*)(void **, const size_t *, const size_t *))dlsym(c.handle, "refshim_gen_run_groups");
         it = g_cache.emplace(key, c).first;
     }
     cl_kernel k = (cl_kernel)calloc(1, sizeof(refshim_kernel));
@@ -227,15 +253,14 @@ cl_kernel ufo_resources_get_kernel_from_source(UfoResources *, const gchar *sour
     return k;
 }
 
-// Kernel files written before the run (the lamino kernels that
-// make_burst_kernels.py generates) are looked up in the cache folder.
 cl_kernel refshim_jit_from_file(const char *file, const char *name, GError **err)
 {
-    std::ifstream f(g_cache_dir + "/" + file);
-    if (!f) return NULL;
-    std::stringstream ss;
-    ss << f.rdbuf();
-    return ufo_resources_get_kernel_from_source(NULL, ss.str().c_str(), name, NULL, err);
+    std::string src;
+    if (!read_kernel_file(file, src)) {
+        g_set_error(err, 0, 0, "kernel file %s not found", file);
+        return NULL;
+    }
+    return ufo_resources_get_kernel_from_source(NULL, src.c_str(), name, NULL, err);
 }
 
 void refshim_jit_dispatch(refshim_kernel *k, guint ndims, const gsize *global, const gsize *local)
@@ -243,6 +268,7 @@ void refshim_jit_dispatch(refshim_kernel *k, guint ndims, const gsize *global, c
     const std::vector<Param> &params = k->jit->params;
     std::vector<void *> a(params.size());
     std::vector<image2d_t> images(params.size());
+    std::vector<image2d_array_t> arrays(params.size());
     std::vector<sampler_t> samplers(params.size());
     // value arguments are copied to 64-byte aligned slots: OpenCL vector types
     // (double3, float8, float16) are over-aligned and AVX loads need it
@@ -259,8 +285,14 @@ void refshim_jit_dispatch(refshim_kernel *k, guint ndims, const gsize *global, c
                 break;
             case 'i': {
                 cl_mem m = *(cl_mem *)slot;
-                images[i] = image2d_t{(const float *)m->host, m->width, m->height};
-                a[i] = &images[i];
+                if (params[i].type == "image2d_array_t") {
+                    const int type = m->channel_type == CL_HALF_FLOAT ? 1 : (m->channel_type == CL_UNSIGNED_INT8 ? 2 : 0);
+                    arrays[i] = image2d_array_t{m->host, m->width, m->height, m->layers, m->channels, type};
+                    a[i] = &arrays[i];
+                } else {
+                    images[i] = image2d_t{(const float *)m->host, m->width, m->height};
+                    a[i] = &images[i];
+                }
                 break;
             }
             case 's':
@@ -275,7 +307,10 @@ void refshim_jit_dispatch(refshim_kernel *k, guint ndims, const gsize *global, c
     size_t l[3] = {1, 1, 1};
     if (local)
         for (guint d = 0; d < ndims; d++) l[d] = local[d];
-    k->jit->prog.run(a.data(), g, l);
+    if (local && k->jit->prog.run_groups)
+        k->jit->prog.run_groups(a.data(), g, l);
+    else
+        k->jit->prog.run(a.data(), g, l);
 }
 
 // ------------------------------------------------------------------ images, samplers, copies

@@ -225,8 +225,12 @@ cl_context ufo_resources_get_context(UfoResources *) { return NULL; }
 
 cl_kernel ufo_resources_get_kernel(UfoResources *, const char *file, const char *name, const char *, GError **err)
 {
-    const size_t fl = file ? strlen(file) : 0;
-    if (fl > 10 && !strcmp(file + fl - 10, "_kernel.cl")) return refshim_jit_from_file(file, name, err);
+    // kernels compiled into this library (ref_kernels.cpp); any other file is
+    // compiled for the CPU when asked for (ref_clc_jit.cpp)
+    static const char *builtin[] = {"backproject.cl", "filter.cl", "fft.cl", "forwardproject.cl", NULL};
+    bool is_builtin = false;
+    for (const char **b = builtin; *b; b++) is_builtin |= file && !strcmp(file, *b);
+    if (!is_builtin) return refshim_jit_from_file(file, name, err);
     cl_kernel k = (cl_kernel)calloc(1, sizeof(refshim_kernel));
     snprintf(k->name, sizeof k->name, "%s", name);
     return k;
@@ -249,6 +253,25 @@ void refshim_buffer_init_bytes(UfoBuffer *b, void *data, size_t bytes, guint n_d
 }
 
 void ufo_buffer_get_requisition(UfoBuffer *b, UfoRequisition *r) { *r = b->req; }
+static size_t buffer_floats(UfoBuffer *b)
+{
+    size_t n = 1;
+    for (guint d = 0; d < b->req.n_dims; d++) n *= b->req.dims[d];
+    return n;
+}
+float *ufo_buffer_get_host_array(UfoBuffer *b, cl_command_queue) { return b->data; }
+float ufo_buffer_min(UfoBuffer *b, cl_command_queue)
+{
+    float m = b->data[0];
+    for (size_t i = 1, n = buffer_floats(b); i < n; i++) m = b->data[i] < m ? b->data[i] : m;
+    return m;
+}
+float ufo_buffer_max(UfoBuffer *b, cl_command_queue)
+{
+    float m = b->data[0];
+    for (size_t i = 1, n = buffer_floats(b); i < n; i++) m = b->data[i] > m ? b->data[i] : m;
+    return m;
+}
 cl_mem ufo_buffer_get_device_array(UfoBuffer *b, cl_command_queue)
 {
     b->mem.is_image = 0;

@@ -69,6 +69,9 @@ cl_kernel ufo_resources_get_kernel_from_source(UfoResources *res, const gchar *s
 void ufo_buffer_get_requisition(UfoBuffer *buf, UfoRequisition *req);
 cl_mem ufo_buffer_get_device_array(UfoBuffer *buf, cl_command_queue q);
 cl_mem ufo_buffer_get_device_image(UfoBuffer *buf, cl_command_queue q);
+gfloat *ufo_buffer_get_host_array(UfoBuffer *buf, cl_command_queue q);
+gfloat ufo_buffer_min(UfoBuffer *buf, cl_command_queue q);
+gfloat ufo_buffer_max(UfoBuffer *buf, cl_command_queue q);
 void ufo_profiler_call(UfoProfiler *p, cl_command_queue q, cl_kernel k, guint ndims, const gsize *global,
                        const gsize *local);
 void ufo_profiler_call_blocking(UfoProfiler *p, cl_command_queue q, cl_kernel k, guint ndims, const gsize *global,

@@ -1,12 +1,13 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-The reference's `filter`, `backproject` and `general-backproject` task sources and its OpenCL
-kernels (with the flat-field and cone-beam weight kernels) are compiled for the CPU by oracle/ref.mk
-(oracle/_ref/libufo_ref.so, see oracle/reference.py); the kernels general-backproject generates at
-run time are compiled when the task asks for them.  This script runs them on seeded inputs and
+The reference's `filter`, `backproject`, `general-backproject`, `lamino-backproject` and
+`stacked-backproject` task sources and its OpenCL kernels (with the flat-field and cone-beam weight kernels) are compiled for
+the CPU by oracle/ref.mk (oracle/_ref/libufo_ref.so, see oracle/reference.py); the kernels
+general-backproject generates at run time, and the lamino kernels its build generates, are compiled
+when the tasks ask for them.  This script runs them on seeded inputs and
 stores inputs and outputs.  Run it where the reference sources are present:
 
-    make -C oracle -f ref.mk && python tests/golden/make_golden.py [fbp|pre|gbp ...]
+    make -C oracle -f ref.mk && python tests/golden/make_golden.py [fbp|pre|gbp|lamino|stacked ...]
 """
 import json
 import math
@@ -19,6 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 sys.path.insert(0, os.path.join(HERE, ".."))
 import gbp_cases  # noqa: E402
+import lamino_cases  # noqa: E402
+import stacked_cases  # noqa: E402
 import oracle  # noqa: E402  (phantom generators only)
 import reference  # noqa: E402
 
@@ -106,11 +109,40 @@ def gbp_golden():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def lamino_golden():
+    """The reference's lamino-backproject task on the cases of tests/lamino_cases.py."""
+    proj = lamino_cases.make_input()
+    out = {"input": proj, "cases": np.array(json.dumps(lamino_cases.CASES))}
+    for c in lamino_cases.CASES:
+        vol = reference.lamino_backproject(proj, c["props"])
+        out["out_" + c["name"]] = vol
+        print("  %-16s %s" % (c["name"], vol.shape))
+    path = os.path.join(HERE, "reference_lamino.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def stacked_golden():
+    """The reference's stacked-backproject task on the cases of tests/stacked_cases.py."""
+    sino = stacked_cases.make_input(oracle)
+    out = {"input": sino, "cases": np.array(json.dumps(stacked_cases.CASES))}
+    for c in stacked_cases.CASES:
+        out["out_" + c["name"]] = reference.stacked_backproject(sino, c["props"])
+        print("  %-10s %s" % (c["name"], out["out_" + c["name"]].shape))
+    path = os.path.join(HERE, "reference_stacked.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["fbp", "pre", "gbp"]
+    which = sys.argv[1:] or ["fbp", "pre", "gbp", "lamino", "stacked"]
     if "fbp" in which:
         main()
     if "pre" in which:
         pre_golden()
     if "gbp" in which:
         gbp_golden()
+    if "lamino" in which:
+        lamino_golden()
+    if "stacked" in which:
+        stacked_golden()

@@ -1,5 +1,6 @@
 """Allocation-free backprojection: ufob_backproject_run_static() through the C
-ABI must give the result of ufob_backproject_run() for the same properties.
+ABI must give the result of ufob_backproject_run() for the same properties,
+and the FP64 oracle's, without allocating device memory.
 
 It exists for callers that cannot call cudaMalloc (memory-pool hosts,
 streaming acquisition); its only scratch is a fixed device
@@ -11,6 +12,7 @@ import numpy as np
 import pytest
 import torch
 
+import oracle
 import ufob
 
 pytestmark = pytest.mark.gpu
@@ -79,6 +81,49 @@ def test_static_matches_allocating_entry_point_twice(cuda):
     torch.cuda.synchronize()
     assert _rel(got1, ref1) < TOL
     assert _rel(got2, ref2) < TOL
+    # and the FP64 oracle of the reference's backproject task on the same rows
+    o1 = oracle.backproject(s1[0].cpu().numpy(), axis_pos=127.25, angle_offset=0.2)
+    assert oracle.rel_l2(got1[0].cpu().numpy(), o1) < TOL
+    o2 = oracle.backproject(s2[1].cpu().numpy(), num_projections=150, offset=30, angle_step=0.02, roi_x=8,
+                            roi_width=96, roi_height=80)
+    assert oracle.rel_l2(got2[1].cpu().numpy(), o2) < TOL
+
+
+def test_static_allocates_nothing(cuda):
+    """Neither the engine's allocation counter nor the device's free memory moves across calls
+    (after the first call on the device, which loads the module and looks up the table)."""
+    L = ufob.lib()
+    L.ufob_device_alloc_count.restype = ctypes.c_uint64
+    rng = np.random.default_rng(5)
+    s = torch.from_numpy(rng.standard_normal((3, 720, 384)).astype(np.float32)).cuda()
+    p = _props(axis_pos=190.5)
+    st, warm = _run_static(p, s, 384)
+    assert st == ufob.OK, ufob.lib().ufob_last_error()
+    out = torch.empty_like(warm)
+    torch.cuda.synchronize()
+    allocs, free = L.ufob_device_alloc_count(), torch.cuda.mem_get_info()[0]
+    fn = L.ufob_backproject_run_static
+    for _ in range(2):
+        st = fn(ctypes.byref(p), s.data_ptr(), ufob.F32, ufob.ROWS, 384, 720, 3, 384, 384 * 720, out.data_ptr(),
+                torch.cuda.current_stream().cuda_stream)
+        assert st == ufob.OK, ufob.lib().ufob_last_error()
+    torch.cuda.synchronize()
+    assert L.ufob_device_alloc_count() == allocs
+    assert torch.cuda.mem_get_info()[0] == free
+    assert torch.equal(out, warm)
+
+
+def test_static_single_sinogram(cuda):
+    """One sinogram of 512 bins x 1536 rows: the allocating entry point splits it into angle groups
+    (partial images summed), the static one runs it whole; equal within round-off."""
+    rng = np.random.default_rng(11)
+    s = torch.from_numpy(rng.standard_normal((1, 1536, 512)).astype(np.float32)).cuda()
+    p = _props(axis_pos=255.5)
+    st, got = _run_static(p, s, 512)
+    assert st == ufob.OK, ufob.lib().ufob_last_error()
+    ref = _run_handle(p, s, 512)
+    assert _rel(got, ref) < TOL
+    assert oracle.rel_l2(got[0].cpu().numpy(), oracle.backproject(s[0].cpu().numpy(), axis_pos=255.5)) < TOL
 
 
 def test_static_pairs_form(cuda):

@@ -8,7 +8,9 @@
 // not take the device-wide synchronisation an allocation can imply while frames
 // are streaming.  For them this file provides
 // ufob_backproject_run_static(): the same kernels, with the only scratch they
-// need -- the angle table -- in a fixed file-scope device array.
+// need -- the angle table -- in a fixed file-scope device array.  The result
+// equals ufob_backproject_run()'s within round-off: a single sinogram is not
+// split into angle groups here.
 //
 // Limits and sharing rules (also stated in ufob.h):
 //  * at most UFOB_STATIC_MAX_ANGLES sinogram rows per call;
@@ -22,6 +24,8 @@
 //    stream capture.
 #include <math.h>
 
+#include <atomic>
+
 #include "ufob_internal.h"
 
 namespace ufob {
@@ -30,7 +34,9 @@ namespace ufob {
 static __device__ __align__(256) float2 g_static_sincos[UFOB_STATIC_MAX_ANGLES];
 
 static constexpr int kMaxDevices = 64;
-static float2 *g_static_ptr[kMaxDevices];  // device address of g_static_sincos per device
+// device address of g_static_sincos per device; host threads that make their
+// first call at the same time both look it up and store the same value
+static std::atomic<float2 *> g_static_ptr[kMaxDevices];
 
 // Per-device set-up: host code may not pass the array's name to a kernel (on
 // the host it is only a stand-in symbol), so look its device address up once
@@ -40,13 +46,15 @@ static ufob_status static_table_address(float2 **out)
     int dev = 0;
     UFOB_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(UFOB_ERR_UNSUPPORTED, "device index %d out of range", dev);
-    if (!g_static_ptr[dev]) {
+    float2 *ptr = g_static_ptr[dev].load(std::memory_order_acquire);
+    if (!ptr) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_sincos);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(static angle table)");
-        g_static_ptr[dev] = reinterpret_cast<float2 *>(p);
+        ptr = reinterpret_cast<float2 *>(p);
+        g_static_ptr[dev].store(ptr, std::memory_order_release);
     }
-    *out = g_static_ptr[dev];
+    *out = ptr;
     return UFOB_OK;
 }
 

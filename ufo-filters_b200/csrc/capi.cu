@@ -45,6 +45,8 @@ ufob_status cuda_fail(cudaError_t e, const char *what)
                 cudaGetErrorString(e), cudaGetErrorName(e));
 }
 
+static std::atomic<uint64_t> g_device_allocs{0};
+
 ufob_status DevBuf::ensure(size_t n)
 {
     if (n <= bytes && ptr) return UFOB_OK;
@@ -55,6 +57,7 @@ ufob_status DevBuf::ensure(size_t n)
         ptr = nullptr;
         return cuda_fail(e, "cudaMalloc");
     }
+    g_device_allocs.fetch_add(1, std::memory_order_relaxed);
     bytes = n;
     return UFOB_OK;
 }
@@ -957,6 +960,7 @@ extern "C" ufob_status ufob_fbp_run_host(ufob_fbp *x, const float *h_sino, uint3
 extern "C" void ufob_fbp_destroy(ufob_fbp *x) { delete x; }
 
 extern "C" uint64_t ufob_launch_count(void) { return g_launches.load(); }
+extern "C" uint64_t ufob_device_alloc_count(void) { return g_device_allocs.load(); }
 
 extern "C" ufob_status ufob_device_status(void)
 {

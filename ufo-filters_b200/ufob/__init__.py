@@ -126,6 +126,7 @@ def lib():
             "ufob_phantom_sinogram": ([vp, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_phantom_stack": ([vp, u32, u32, u32, u32, d, d, d, vp, vp], i),
             "ufob_launch_count": ([], ctypes.c_uint64),
+            "ufob_device_alloc_count": ([], ctypes.c_uint64),
             "ufob_forwardproject": ([vp, u32, u32, d, d, vp, vp], i),
             "ufob_phantom_images": ([vp, vp, u32, u32, d, d, i, vp, vp], i),
             "ufob_measure_peaks": ([ctypes.POINTER(d), ctypes.POINTER(d)], i),
@@ -869,6 +870,11 @@ def phantom_stack(ellipsoids, width, n_angles, nslices, angle_step=None, axis=No
 
 def launch_count():
     return int(lib().ufob_launch_count())
+
+
+def device_alloc_count():
+    """Device allocations (cudaMalloc) the engine has made in this process so far."""
+    return int(lib().ufob_device_alloc_count())
 
 
 def measure_peaks():
