@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-slices", type=int, default=0, help="0 = as many as host memory allows (<= --slices)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the CPU baseline sample")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other four workloads' table")
     return ap.parse_args()
 
 
@@ -144,11 +144,14 @@ class ClockSampler:
 
 # ----------------------------------------------------------------------------- CPU leg (oracle)
 
-def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
-    """CPU baseline and FP64 error reference.  The oracle (C restatement of the
+def cpu_leg(stack_host_slices, slice_ids, roi, P, W, gpu_rois):
+    """CPU baseline and error references.  The oracle (C restatement of the
     reference's fft ! filter ! ifft ! backproject, OpenMP on all host cores)
-    reconstructs a fixed ROI of the sampled slices in FP64; its wall time gives
-    the CPU GUPS and its output is the FP64 reference for the error report."""
+    reconstructs a fixed ROI of the sampled slices in FP64: the reference for
+    the error report.  The reference's own filter/backproject code compiled for
+    the CPU reconstructs the same ROI: its wall time gives the CPU GUPS and its
+    output the second error reference (the plain form must match it within
+    1e-4 relative L2)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     import oracle
@@ -159,16 +162,26 @@ def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
         filt = oracle.fft_filter_ifft(s).astype(np.float32)
         refs.append(oracle.backproject(filt, roi_x=rx, roi_y=ry, roi_width=rw, roi_height=rh))
     # timed: the reference's own filter/backproject code on the host cores where its CPU build
-    # is present, else the oracle
+    # is present, else the oracle, on the whole slices (about 10 s of CPU work: 4 x 2048^2 x 1500
+    # updates at ~2 GUPS); the error ROI is cut from them
     impl = reference if reference.available() else oracle
+    tw = W
+    tx, ty = min(max(rx - (tw - rw) // 2, 0), W - tw), min(max(ry - (tw - rh) // 2, 0), W - tw)
+    outs = []
     t0 = time.perf_counter()
     for s in stack_host_slices:
         filt = impl.fft_filter_ifft(s).astype(np.float32)
-        impl.backproject(filt, roi_x=rx, roi_y=ry, roi_width=rw, roi_height=rh)
+        big = impl.backproject(filt, roi_x=tx, roi_y=ty, roi_width=tw, roi_height=tw)
+        outs.append(big[ry - ty:ry - ty + rh, rx - tx:rx - tx + rw])
     dt = time.perf_counter() - t0
-    updates = len(stack_host_slices) * rw * rh * P
-    errors = {k: float(np.linalg.norm(np.stack(v) - np.stack(refs)) / np.linalg.norm(np.stack(refs)))
-              for k, v in gpu_rois.items()}
+    updates = len(stack_host_slices) * tw * tw * P
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.stack(a) - np.stack(b)) / np.linalg.norm(np.stack(b)))
+    errors = {k: {"rel_l2_vs_fp64": rel(v, refs)} for k, v in gpu_rois.items()}
+    if impl is reference:
+        for k, v in gpu_rois.items():
+            errors[k]["rel_l2_vs_reference"] = rel(v, outs)
     cores = os.cpu_count()
     try:
         cores = len(os.sched_getaffinity(0))
@@ -179,7 +192,7 @@ def cpu_leg(stack_host_slices, slice_ids, roi, P, W, target_s, gpu_rois):
             else "FP64 oracle")
     return {"value": updates / dt / 1e9, "unit": "GUPS", "cores": cores, "kind": kind,
             "sample": "%s: fft/filter/ifft of %d full slices + backprojection of a %dx%d ROI (%d angles), "
-                      "%.2e updates, %.1f s" % (what, len(stack_host_slices), rw, rh, P, updates, dt)}, errors
+                      "%.2e updates, %.1f s" % (what, len(stack_host_slices), tw, tw, P, updates, dt)}, errors
 
 
 def reference_arm(args):
@@ -239,6 +252,178 @@ def read_profile_traffic(name):
         return None
     m = re.search(r"dram_bytes_per_update:\s*([0-9.eE+-]+)", text)
     return float(m.group(1)) if m else None
+
+
+def _event_ms(torch, fn, reps):
+    """Mean CUDA-event time (ms) of reps calls after one warm-up call, on torch's current
+    stream (the stream the engine's Python objects launch on)."""
+    fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+C2_GEOMETRIES = {"cone": {"source-position-y": -800.0, "detector-position-y": 200.0},
+                 "lamino_30deg": {"axis-angle-x": math.pi / 6},
+                 "parallel": {}}
+
+
+def run_configs(ufob, torch, dev, seed):
+    """The other four workloads on this GPU, timed with CUDA events: one 512^2
+    slice (512 angles), general backprojection of 1024 projections of 1024^2
+    into 512^3 (cone, laminography 30 degrees, parallel), the 64-job uneven
+    batch, and the learned 90-angle path against dense FBP.  Returns the table
+    and the host copies of sampled outputs that the CPU leg checks."""
+    import numpy as np
+    from ufob.cnn import PairMaker, SparseViewNet, random_ellipses, rel_l2
+    from ufob.train_cnn import time_paths
+    table, checks = {}, {}
+
+    # configuration 0: one 512^2 slice from 512 angles, axis 255.5 (10 random ellipses)
+    W0 = P0 = 512
+    sino0 = ufob.phantom_sinogram(random_ellipses(seed), W0, P0, axis=255.5)
+    c0, outs0 = {}, {}
+    for name, storage in (("plain_fp32", ufob.F32), ("fp16_storage", ufob.F16)):
+        fbp = ufob.FBP(bp_props={"axis_pos": 255.5}, storage=storage)
+        img = fbp.process(sino0)
+        ms = _event_ms(torch, lambda: fbp.process(sino0, out=img), 200)
+        c0[name] = {"us_per_slice": round(ms * 1e3, 2), "gups": round(W0 * W0 * P0 / ms / 1e6, 1)}
+        outs0[name] = img.double().cpu().numpy()
+    table["c0_single_slice"] = dict(workload="fft ! filter ! ifft ! backproject of one 512 px x 512 angle "
+                                             "sinogram (10 random ellipses), axis 255.5, per call", **c0)
+    checks["c0"] = (sino0.cpu().numpy(), outs0)
+    del sino0
+
+    # configuration 2: general-backproject, 1024 projections of 1024^2 over 360 degrees -> 512^3
+    n_proj, det, vol = 1024, 1024, 512
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    proj = torch.rand(n_proj, det, det, device=dev, generator=gen)
+    h, q = vol / 2.0, 64
+    base = {"center-position-x": det / 2.0, "center-position-z": det / 2.0,
+            "x-region": (-h, h, 1.0), "y-region": (-h, h, 1.0), "region": (-h, h, 1.0)}
+    c2, rois2 = {}, {}
+    for gname, geom in C2_GEOMETRIES.items():
+        for ct in ("float", "half"):
+            t = ufob.GeneralBackprojectTask(num_projections=n_proj)
+            t.set_property("compute-type", ct)
+            for k, v in list(base.items()) + list(geom.items()):
+                t.set_property(k, v)
+            v = t.process(proj)
+            ms = _event_ms(torch, lambda: t.process(proj, out=v), 2)
+            c2["%s_%s" % (gname, ct)] = {"ms": round(ms, 2), "gups": round(float(vol) ** 3 * n_proj / ms / 1e6, 1)}
+            rois2["%s_%s" % (gname, ct)] = v[vol // 2, vol // 2 - q:vol // 2 + q,
+                                              vol // 2 - q:vol // 2 + q].double().cpu().numpy()
+            del t, v
+    table["c2_general_backproject"] = dict(
+        workload="general-backproject, %d projections of %d^2 over 360 degrees -> %d^3 (seeded uniform random "
+                 "projections; the rate does not depend on the values), exact FP32 interpolation weights; "
+                 "compute-type float and half (FP16 samples, FP32 arithmetic)" % (n_proj, det, vol), **c2)
+    checks["c2"] = (proj.cpu().numpy(), base, q, rois2)
+    del proj
+    torch.cuda.empty_cache()
+
+    # configuration 3: 64 uneven parallel-beam jobs in one persistent graph-captured launch pair
+    rng = np.random.default_rng(seed)
+    jobs, upd = [], 0
+    for j in range(64):
+        W = int(rng.choice([256, 512, 1024, 1536, 2048]))
+        P = int(rng.integers(180, 1801))
+        jobs.append(dict(sino=ufob.phantom_sinogram(random_ellipses(seed * 1000 + j), W, P),
+                         out=torch.empty((W, W), device=dev)))
+        upd += W * W * P
+    c3, outs3 = {}, {}
+    sizes = [j["sino"].shape[-1] ** 2 * j["sino"].shape[-2] for j in jobs]
+    i_small, i_big = int(np.argmin(sizes)), int(np.argmax(sizes))
+    i_1536 = next((i for i, j in enumerate(jobs) if j["sino"].shape[-1] == 1536), i_big)
+    picks = sorted({i_small, i_big, i_1536})
+    # checked region of each picked job: the whole slice up to 256^2, else the 128^2 block (on a
+    # 64-pixel grid) with the most energy in a first FP32 run, so that an empty patch of the
+    # phantom cannot inflate the relative error
+    ufob.Batch(storage=ufob.F32).run(jobs)
+    rois3 = []
+    for i in picks:
+        W = jobs[i]["sino"].shape[-1]
+        if W <= 256:
+            rois3.append((0, 0, W))
+            continue
+        img = jobs[i]["out"]
+        e = torch.nn.functional.avg_pool2d((img * img)[None, None], 128, stride=64)[0, 0]
+        k = int(torch.argmax(e))
+        rois3.append(((k % e.shape[1]) * 64, (k // e.shape[1]) * 64, 128))
+    for name, storage in (("fp32", ufob.F32), ("fp16", ufob.F16), ("bf16", ufob.BF16)):
+        b = ufob.Batch(storage=storage)
+        ms = _event_ms(torch, lambda: b.run(jobs), 3)
+        c3[name] = {"ms": round(ms, 2), "gups": round(upd / ms / 1e6, 1), "tile_variant": b.variant()}
+        outs3[name] = [jobs[i]["out"][y:y + n, x:x + n].double().cpu().numpy()
+                       for i, (x, y, n) in zip(picks, rois3)]
+        del b
+    table["c3_uneven_batch"] = dict(workload="64 parallel-beam jobs, widths from {256,512,1024,1536,2048}, 180-1800 "
+                                             "angles (seed %d), random-ellipse phantoms, %.3e updates" % (seed, upd),
+                                    **c3)
+    checks["c3"] = ([jobs[i]["sino"].cpu().numpy() for i in picks], rois3, outs3)
+    del jobs
+    torch.cuda.empty_cache()
+
+    # configuration 4: learned 90-angle path (shipped weights) against dense 1800-angle FBP
+    maker = PairMaker()
+    net = SparseViewNet.pretrained()
+    seeds = list(range(1_000_000, 1_000_064))
+    imgs = maker.phantoms(seeds)
+    x = maker.fbp_sparse.process(maker.sinograms(imgs, maker.sparse))
+    y = maker.fbp_dense.process(maker.sinograms(imgs, maker.dense))
+    table["c4_learned_sparse_view"] = {
+        "workload": "90-angle 512 px FBP + 4-level CNN (32/64/128/256 ch, BF16 tensor cores) vs 1800-angle FBP, "
+                    "shipped weights, 64 held-out phantoms (seeds 1e6..)",
+        "plain_fbp90_rel_l2_vs_1800": round(float(rel_l2(x, y).mean()), 5),
+        "cnn_rel_l2_vs_1800": round(float(rel_l2(net.forward(x), y).mean()), 5),
+        "time_per_slice": [time_paths(net, maker, B=b) for b in (64, 128, 256)]}
+    del imgs, x, y, net, maker
+    torch.cuda.empty_cache()
+    return table, checks
+
+
+def config_errors(checks):
+    """CPU leg of the other workloads: relative L2 errors of the sampled GPU outputs
+    against the FP64 oracle and, for the one-slice FBP, the reference's own CPU build."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import reference
+    err = {}
+    sino0, outs0 = checks["c0"]
+    ref64 = oracle.fbp(sino0, axis_pos=255.5)
+    err["c0_single_slice"] = {k: {"rel_l2_vs_fp64": oracle.rel_l2(v, ref64)} for k, v in outs0.items()}
+    if reference.available():
+        refc = reference.backproject(reference.fft_filter_ifft(sino0).astype(np.float32), axis_pos=255.5)
+        for k, v in outs0.items():
+            err["c0_single_slice"][k]["rel_l2_vs_reference"] = oracle.rel_l2(v, refc)
+    proj, base, q, rois2 = checks["c2"]
+    err["c2_general_backproject"] = {}
+    for gname, geom in C2_GEOMETRIES.items():
+        kw = {k: v for k, v in list(base.items()) + list(geom.items()) if "region" not in k}
+        ref = oracle.general_backproject(proj, proj.shape[0], region=(0.0, 1.0, 1.0), x_region=(-q, q, 1.0),
+                                         y_region=(-q, q, 1.0), **kw)[0]
+        for ct in ("float", "half"):
+            err["c2_general_backproject"]["%s_%s" % (gname, ct)] = {
+                "rel_l2_vs_fp64": oracle.rel_l2(rois2["%s_%s" % (gname, ct)], ref),
+                "sample": "central slice, %dx%d voxels" % (2 * q, 2 * q)}
+    sinos3, rois3, outs3 = checks["c3"]
+    refs3 = []
+    for s, (x, y, n) in zip(sinos3, rois3):
+        W = s.shape[-1]
+        N = 1 << (W - 1).bit_length()
+        refs3.append(oracle.backproject(oracle.fft_filter_ifft(s, size_x=N, crop_width=W).astype(np.float32),
+                                        roi_x=x, roi_y=y, roi_width=n, roi_height=n))
+    err["c3_uneven_batch"] = {k: {"rel_l2_vs_fp64_max": max(oracle.rel_l2(a, b) for a, b in zip(v, refs3)),
+                                  "sample": "jobs (angles, width) %s, regions (x, y, side) %s"
+                                            % ([tuple(s.shape) for s in sinos3], rois3)}
+                              for k, v in outs3.items()}
+    return err
 
 
 def main():
@@ -316,10 +501,9 @@ def main():
     cpu = None
     if rank == 0:
         host_slices = [stack[i].cpu().numpy() for i in slice_ids]
-        cpu, errs = cpu_leg(host_slices, slice_ids, roi, P, W, args.cpu_seconds,
-                            {k: v["_rois"] for k, v in forms.items()})
+        cpu, errs = cpu_leg(host_slices, slice_ids, roi, P, W, {k: v["_rois"] for k, v in forms.items()})
         for k in forms:
-            forms[k]["rel_l2_vs_fp64"] = errs[k]
+            forms[k].update(errs[k])
     for k in forms:
         forms[k].pop("_rois")
 
@@ -344,14 +528,13 @@ def main():
         h_in = torch.empty((nz_e2e, P, W), dtype=torch.float32, pin_memory=True)
         h_in.copy_(stack[:nz_e2e])
         h_out = torch.empty((nz_e2e, W, W), dtype=torch.float32, pin_memory=True)
-        del stack
-        del vol
+        stack = vol = None
         torch.cuda.empty_cache()
         fbp = ufob.FBP(bp_props={"axis_pos": W / 2.0, "compensated": 0 if storage == ufob.F32 else 1},
                        storage=storage)
         fbp.process_host(h_in[:min(16, nz_e2e)], out=h_out[:min(16, nz_e2e)], slices_per_chunk=16)
         times = []
-        for i in range(max(1, min(args.steps, 2))):
+        for i in range(args.steps):
             barrier()
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -364,6 +547,22 @@ def main():
                "slices": nz_e2e, "s_per_step": dt,
                "api": "ufob_fbp_run_host (C ABI), pinned host buffers, 64-slice chunks (16-slice first and last) on two streams"}
         del fbp, h_in, h_out
+
+    # the other four workloads (one-GPU configurations), timed on this GPU after the main arm, with
+    # their own clock record; errors from the CPU leg
+    configs = None
+    if world == 1 and not args.no_configs:
+        stack = vol = None
+        torch.cuda.empty_cache()
+        sampler = ClockSampler(gpu_id)
+        sampler.start()
+        table, checks = run_configs(ufob, torch, dev, args.seed)
+        table["clocks"] = sampler.stop()
+        ufob.device_status()
+        for k, v in config_errors(checks).items():
+            for form, e in v.items():
+                table[k][form].update(e)
+        configs = table
 
     # roofline of the dominant kernel (backprojection)
     bp_ms, bp_n = chosen["kernel_ms_per_step"]["backproject"], chosen["kernel_launches_per_step"]["backproject"]
@@ -415,6 +614,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": int(round(chosen["launches_per_step"] * args.steps)),
             "clocks": clk,
+            "configs": configs,
         }
         print(json.dumps(line), flush=True)
     udist.finish(ctx)

@@ -143,16 +143,36 @@ def test_single_sinogram_angle_groups(cuda, dtype, tol):
     noise sinogram, whose slice is small against its terms."""
     rng = np.random.default_rng(21)
     W, P = 512, 1536
+    # the engine's choice (capi.cu split_groups): 16 x 6 tiles of 32x96 pixels per group, split
+    # into 2, 4 or 8 groups when that lowers the busiest SM's share over the average by > 0.05
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    tiles = ((W + 31) // 32) * ((W + 95) // 96)
+
+    def imbalance(k):
+        per_sm = tiles * k / sms
+        return math.ceil(per_sm) / per_sm
+    groups, best = 1, imbalance(1)
+    for k in (2, 4, 8):
+        if P % k or P // k < 32:
+            break
+        if imbalance(k) < best - 0.05:
+            groups, best = k, imbalance(k)
+    assert groups > 1, "the case must exercise the angle-group split on this GPU (%d SMs)" % sms
     raw = rng.standard_normal((P, W)).astype(np.float32)
     f = ufob.FilterTask()
     ref = oracle.backproject(oracle.fft_filter_ifft(raw).astype(np.float32))
     if dtype == ufob.F32:
-        filt = f.process(torch.from_numpy(raw).cuda())
-        got = ufob.BackprojectTask().process(filt).cpu().numpy()
-        unsplit = ufob.BackprojectTask(tile=8).process(filt).cpu().numpy()
+        src, kw = f.process(torch.from_numpy(raw).cuda()), {}
     else:
-        pairs = f.process(torch.from_numpy(raw).cuda(), dtype=dtype, layout=ufob.PAIRS)
-        got = ufob.BackprojectTask().process(pairs, dtype=dtype, layout=ufob.PAIRS, width=W).cpu().numpy()
-        unsplit = ufob.BackprojectTask(tile=8).process(pairs, dtype=dtype, layout=ufob.PAIRS, width=W).cpu().numpy()
+        src = f.process(torch.from_numpy(raw).cuda(), dtype=dtype, layout=ufob.PAIRS)
+        kw = dict(dtype=dtype, layout=ufob.PAIRS, width=W)
+    torch.cuda.synchronize()
+    n0 = ufob.launch_count()
+    got = ufob.BackprojectTask().process(src, **kw).cpu().numpy()
+    n1 = ufob.launch_count()
+    unsplit = ufob.BackprojectTask(tile=8).process(src, **kw).cpu().numpy()
+    n2 = ufob.launch_count()
+    # the split run adds exactly one launch: the ordered sum of the partial images
+    assert (n1 - n0) == (n2 - n1) + 1
     assert oracle.rel_l2(got, ref) < tol
     assert oracle.rel_l2(got, unsplit) < 1e-5

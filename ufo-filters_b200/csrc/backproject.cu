@@ -963,11 +963,8 @@ static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32
 {
     using Sh = BPShape<TX, TY, ZT, A, S>;
     auto kern = k_bp_linear<TX, TY, ZT, A, S, KIND, KAHAN>;
-    static bool attr = false;
-    if (!attr) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(kern, (int)Sh::kSmem, attr_devs));
     CUtensorMap map;
     UFOB_TRY(make_sino_map(&map, d_sino, elems, g.P, g.nz, pitch, slice_pitch, Sh::kWin, ZT));
     BPArgs a;
@@ -1090,11 +1087,8 @@ static ufob_status launch_quads_t(const BPGeometry &g, const void *d_sino, uint3
 {
     using Sh = BPQShape<TX, TY, ZT, A, S>;
     auto kern = k_bp_quads<TX, TY, ZT, A, S, ACC, KAHAN>;
-    static bool attr = false;
-    if (!attr) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(kern, (int)Sh::kSmem, attr_devs));
     CUtensorMap map;
     UFOB_TRY(make_quad_map(&map, d_sino, g.W + 1, g.P, (g.nz + 3) / 4, pitch, group_pitch, Sh::kWin, Sh::kGroups));
     BPArgs a;

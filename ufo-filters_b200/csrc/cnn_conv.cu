@@ -383,12 +383,8 @@ ufob_status conv3x3_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *w, cons
 {
     if (Cin % 16 || Cout % 16 || Cin < 16 || Cout < 16 || Cin > 256 || Cout > 256 || (Cin > 64 && Cin % 64))
         return fail(UFOB_ERR_INVALID, "conv3x3: channels must be multiples of 16 in [16, 256] (Cin > 64: of 64)");
-    static bool attr = false;
-    if (!attr) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)conv_smem_bytes()));
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(k_conv3x3, (int)conv_smem_bytes(), attr_devs));
     ConvArgs a;
     a.in = in;
     a.w = w;
@@ -416,12 +412,8 @@ ufob_status conv3x3_wgrad_launch(const __nv_bfloat16 *in, const __nv_bfloat16 *d
 {
     if (Cin % 16 || Cout % 16 || Cin < 16 || Cout < 16 || Cin > 256 || Cout > 256)
         return fail(UFOB_ERR_INVALID, "conv3x3 wgrad: channels must be multiples of 16 in [16, 256]");
-    static bool attr = false;
-    if (!attr) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(k_conv3x3_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)conv_smem_bytes()));
-        attr = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(k_conv3x3_wgrad, (int)conv_smem_bytes(), attr_devs));
     const long long npix = (long long)NB * H * W;
     // about two waves of CTAs over (pixel ranges x 9 taps x channel tiles)
     const int mt = (Cout + 127) / 128;

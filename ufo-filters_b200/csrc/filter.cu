@@ -768,12 +768,9 @@ static ufob_status launch_rows_t(const FilterPlan &plan, const RowSource &src, u
     const uint32_t N = plan.nfft;
     const size_t smem = sizeof(float2) * (3 * (size_t)N + N / 2 + 1);
     auto kern = k_filter_rows<OUT, PRE>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(sizeof(float2) * (3 * (size_t)kMaxFusedFFT + kMaxFusedFFT / 2 + 1))));
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(
+        kern, (int)(sizeof(float2) * (3 * (size_t)kMaxFusedFFT + kMaxFusedFFT / 2 + 1)), attr_devs));
     const int log2N = ilog2(N);
     int per_sm = 0;
     UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFilterThreads, smem));
@@ -797,11 +794,8 @@ static ufob_status launch_fast_t(const FilterPlan &plan, const RowSource &src, u
     constexpr uint32_t N = 1u << LOGN, TEAMS = kFastThreads / (N / 16);
     const size_t smem = sizeof(float2) * (pass_twiddle_count(N) + N / 2 + 2 + (size_t)TEAMS * 2 * N);
     auto kern = k_filter_fast<OUT, PRE, LOGN>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        UFOB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(kern, (int)smem, attr_devs));
     int per_sm = 0;
     UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, smem));
     if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -25,6 +26,23 @@ void note_launch(uint64_t n = 1);  // count kernels launched (ufob_launch_count)
         cudaError_t _e = (expr);                                  \
         if (_e != cudaSuccess) return ::ufob::cuda_fail(_e, #expr); \
     } while (0)
+
+// Raises a kernel's dynamic shared-memory limit on the current device, once per device: the
+// attribute belongs to the device's context, so a process that drives several GPUs sets it on
+// each of them.  `done` is the calling launcher's own record, one bit per device ordinal < 64
+// (higher ordinals set the attribute on every call).
+template <typename K>
+inline cudaError_t smem_limit_per_device(K kern, int bytes, std::atomic<uint64_t> &done)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 #define UFOB_TRY(expr)                        \
     do {                                      \
