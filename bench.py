@@ -308,21 +308,26 @@ def run_configs(ufob, torch, dev, seed):
             "x-region": (-h, h, 1.0), "y-region": (-h, h, 1.0), "region": (-h, h, 1.0)}
     c2, rois2 = {}, {}
     for gname, geom in C2_GEOMETRIES.items():
-        for ct in ("float", "half"):
+        # float: TMA-staged detector windows (the default); float_texture: the texture-gather
+        # kernel; half: FP16 samples through texture gathers
+        for form, ct, staging in (("float", "float", "auto"), ("float_texture", "float", "texture"),
+                                  ("half", "half", "auto")):
             t = ufob.GeneralBackprojectTask(num_projections=n_proj)
             t.set_property("compute-type", ct)
+            t.set_property("staging", staging)
             for k, v in list(base.items()) + list(geom.items()):
                 t.set_property(k, v)
             v = t.process(proj)
             ms = _event_ms(torch, lambda: t.process(proj, out=v), 2)
-            c2["%s_%s" % (gname, ct)] = {"ms": round(ms, 2), "gups": round(float(vol) ** 3 * n_proj / ms / 1e6, 1)}
-            rois2["%s_%s" % (gname, ct)] = v[vol // 2, vol // 2 - q:vol // 2 + q,
-                                              vol // 2 - q:vol // 2 + q].double().cpu().numpy()
+            key = "%s_%s" % (gname, form)
+            c2[key] = {"ms": round(ms, 2), "gups": round(float(vol) ** 3 * n_proj / ms / 1e6, 1)}
+            rois2[key] = v[vol // 2, vol // 2 - q:vol // 2 + q, vol // 2 - q:vol // 2 + q].double().cpu().numpy()
             del t, v
     table["c2_general_backproject"] = dict(
         workload="general-backproject, %d projections of %d^2 over 360 degrees -> %d^3 (seeded uniform random "
                  "projections; the rate does not depend on the values), exact FP32 interpolation weights; "
-                 "compute-type float and half (FP16 samples, FP32 arithmetic)" % (n_proj, det, vol), **c2)
+                 "compute-type float with TMA-staged detector windows (default) and with texture gathers, "
+                 "compute-type half (FP16 samples, FP32 arithmetic)" % (n_proj, det, vol), **c2)
     checks["c2"] = (proj.cpu().numpy(), base, q, rois2)
     del proj
     torch.cuda.empty_cache()
@@ -408,9 +413,9 @@ def config_errors(checks):
         kw = {k: v for k, v in list(base.items()) + list(geom.items()) if "region" not in k}
         ref = oracle.general_backproject(proj, proj.shape[0], region=(0.0, 1.0, 1.0), x_region=(-q, q, 1.0),
                                          y_region=(-q, q, 1.0), **kw)[0]
-        for ct in ("float", "half"):
-            err["c2_general_backproject"]["%s_%s" % (gname, ct)] = {
-                "rel_l2_vs_fp64": oracle.rel_l2(rois2["%s_%s" % (gname, ct)], ref),
+        for form in ("float", "float_texture", "half"):
+            err["c2_general_backproject"]["%s_%s" % (gname, form)] = {
+                "rel_l2_vs_fp64": oracle.rel_l2(rois2["%s_%s" % (gname, form)], ref),
                 "sample": "central slice, %dx%d voxels" % (2 * q, 2 * q)}
     sinos3, rois3, outs3 = checks["c3"]
     refs3 = []

@@ -262,7 +262,12 @@ ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double value);
  * or "texture" (the texture unit's linear filter with 8-bit weights, as the reference samples
  * on a GPU; FP32 compute type).  compute-type "half" stores the projection samples as FP16
  * (texture gathers of 16-bit texels run at twice the FP32 rate) and keeps coordinates, weights
- * and sums in FP32; the reference's half type also computes those in half precision. */
+ * and sums in FP32; the reference's half type also computes those in half precision.  The
+ * engine property "staging": "auto" (default) stages each projection's detector window in
+ * shared memory by TMA where the geometry lets a z-column of voxels share its detector column
+ * (float compute/result/store types, exact weights, parameter z, clamp addressing, width a
+ * multiple of 4), else samples through texture gathers; "texture" always uses the gathers.
+ * Both give the same values to FP32 rounding. */
 ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value);
 ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n);
 /* setup(): validates num-projections, gray mapping; builds angle tables. */

@@ -32,78 +32,10 @@
 #include <algorithm>
 #include <cmath>
 
+#include "tma.cuh"
 #include "ufob_internal.h"
 
 namespace ufob {
-
-// ------------------------------------------------------------------ PTX helpers
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ uint64_t global_timer_ns()
-{
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Wait for phase `parity` of `bar`, giving up after `limit_ns`.  The timer is
-// read only every 256 polls so that its latency does not delay the wake-up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
-{
-    uint64_t t0 = 0;
-    for (uint32_t i = 1;; i++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 255u) == 0) {
-            const uint64_t t = global_timer_ns();
-            if (!t0)
-                t0 = t;
-            else if (t - t0 > limit_ns)
-                return false;
-        }
-    }
-}
-
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-        "[%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_barrier_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-static constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s
-static constexpr int kErrTmaTimeout = 0x1001;
 
 // ------------------------------------------------------------------ tensor maps
 
@@ -136,6 +68,26 @@ ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, ui
     if (r != CUDA_SUCCESS)
         return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): elems=%u P=%u nz=%u pitch=%u box=%u,%u",
                     (int)r, elems, P, nz, pitch, box_x, box_z);
+    return UFOB_OK;
+}
+
+// 3-D map over [n][H][W] 4-byte elements (rows `pitch` elements apart, planes `plane` elements
+// apart); box = (box_w, box_h, 1).  Coordinates outside the array read 0.
+ufob_status make_image_map(CUtensorMap *map, const void *base, uint32_t W, uint32_t H, uint32_t n, uint64_t pitch,
+                           uint64_t plane, uint32_t box_w, uint32_t box_h)
+{
+    auto fn = encode_fn();
+    if (!fn) return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[3] = {W, H, n};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)plane * 4};
+    cuuint32_t box[3] = {box_w, box_h, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(UFOB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d): image %ux%ux%u pitch=%llu box=%ux%u", (int)r,
+                    W, H, n, (unsigned long long)pitch, box_w, box_h);
     return UFOB_OK;
 }
 

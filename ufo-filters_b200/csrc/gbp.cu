@@ -31,9 +31,11 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 #include <string>
 
+#include "tma.cuh"
 #include "ufob_internal.h"
 
 namespace ufob {
@@ -56,25 +58,25 @@ __device__ __forceinline__ double fmaf_ct(double a, double b, double c) { return
 struct d3 {
     double x, y, z;
 };
-__device__ __forceinline__ d3 rx(double s, double c, d3 p) { return {p.x, c * p.y - s * p.z, s * p.y + c * p.z}; }
-__device__ __forceinline__ d3 ry(double s, double c, d3 p) { return {c * p.x + s * p.z, p.y, -s * p.x + c * p.z}; }
-__device__ __forceinline__ d3 rz(double s, double c, d3 p) { return {c * p.x - s * p.y, s * p.x + c * p.y, p.z}; }
+__host__ __device__ inline d3 rx(double s, double c, d3 p) { return {p.x, c * p.y - s * p.z, s * p.y + c * p.z}; }
+__host__ __device__ inline d3 ry(double s, double c, d3 p) { return {c * p.x + s * p.z, p.y, -s * p.x + c * p.z}; }
+__host__ __device__ inline d3 rz(double s, double c, d3 p) { return {c * p.x - s * p.y, s * p.x + c * p.y, p.z}; }
 
 // 4-component row vectors of affine forms in X = (ix, iy, z, 1)
 struct Row {
     double a[4];
 };
-__device__ __forceinline__ Row rsc(Row r, double k)
+__host__ __device__ inline Row rsc(Row r, double k)
 {
     for (int i = 0; i < 4; i++) r.a[i] *= k;
     return r;
 }
-__device__ __forceinline__ Row radd(Row p, Row q)
+__host__ __device__ inline Row radd(Row p, Row q)
 {
     for (int i = 0; i < 4; i++) p.a[i] += q.a[i];
     return p;
 }
-__device__ __forceinline__ Row rconst(double k)
+__host__ __device__ inline Row rconst(double k)
 {
     Row r = {{0.0, 0.0, 0.0, k}};
     return r;
@@ -83,7 +85,7 @@ struct Rows3 {
     Row x, y, z;
 };
 // rotate a triple of rows (a linear map applied component-wise)
-__device__ __forceinline__ Rows3 rot_rows(int axis, double s, double c, Rows3 p)
+__host__ __device__ inline Rows3 rot_rows(int axis, double s, double c, Rows3 p)
 {
     Rows3 o = p;
     if (axis == 0) {
@@ -99,18 +101,13 @@ __device__ __forceinline__ Rows3 rot_rows(int axis, double s, double c, Rows3 p)
     return o;
 }
 
-// One table entry per (slice-or-0, projection).  geom: [n_proj][GC_NCOLS]
-// FP64; when param_col >= 0 the column is replaced by slice_values[slice].
-__global__ void k_gbp_tables(const double *__restrict__ geom, uint32_t n_proj, uint32_t n_tab_slices, int param_col,
-                             const double *__restrict__ slice_values, int flags, double x0, double dxs, double y0,
-                             double dys, float *__restrict__ tf, double *__restrict__ td)
+// The table of one projection (and slice): the chain of make_transformations
+// (src/ufo-general-backproject-task.c:909-1048) for geometry row g [GC_NCOLS],
+// as rows Nu, Nv, D, C of affine forms in X = (ix, iy, z, 1) and K, in FP64.
+// Shared by the device table builder and the host's staging plan.
+__host__ __device__ inline void gbp_table_entry(const double *g, int flags, double x0, double dxs, double y0,
+                                                double dys, double vals[kTab])
 {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t sl = blockIdx.y;
-    if (p >= n_proj || sl >= n_tab_slices) return;
-    double g[GC_NCOLS];
-    for (int i = 0; i < GC_NCOLS; i++) g[i] = geom[(size_t)p * GC_NCOLS + i];
-    if (param_col >= 0) g[param_col] = slice_values[sl];
     const bool parallel = flags & GF_PARALLEL, perp = flags & GF_PERPENDICULAR;
     const double sx = g[GC_SRC_X], sy = g[GC_SRC_Y], sz = g[GC_SRC_Z];
     const double dx = g[GC_DET_X], dy = g[GC_DET_Y], dz = g[GC_DET_Z];
@@ -203,9 +200,26 @@ __global__ void k_gbp_tables(const double *__restrict__ geom, uint32_t n_proj, u
         C = radd(rconst(sy), rsc(M.y, -1.0));  // s.y - V.y
         K = sy - dy;
     }
+    const double v[kTab] = {Nu.a[0], Nu.a[1], Nu.a[2], Nu.a[3], Nv.a[0], Nv.a[1], Nv.a[2], Nv.a[3],
+                            D.a[0],  D.a[1],  D.a[2],  D.a[3],  C.a[0],  C.a[1],  C.a[2],  C.a[3], K, 0.0, 0.0, 0.0};
+    for (int i = 0; i < kTab; i++) vals[i] = v[i];
+}
+
+// One table entry per (slice-or-0, projection).  geom: [n_proj][GC_NCOLS]
+// FP64; when param_col >= 0 the column is replaced by slice_values[slice].
+__global__ void k_gbp_tables(const double *__restrict__ geom, uint32_t n_proj, uint32_t n_tab_slices, int param_col,
+                             const double *__restrict__ slice_values, int flags, double x0, double dxs, double y0,
+                             double dys, float *__restrict__ tf, double *__restrict__ td)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t sl = blockIdx.y;
+    if (p >= n_proj || sl >= n_tab_slices) return;
+    double g[GC_NCOLS];
+    for (int i = 0; i < GC_NCOLS; i++) g[i] = geom[(size_t)p * GC_NCOLS + i];
+    if (param_col >= 0) g[param_col] = slice_values[sl];
+    double vals[kTab];
+    gbp_table_entry(g, flags, x0, dxs, y0, dys, vals);
     const size_t o = ((size_t)sl * n_proj + p) * kTab;
-    double vals[kTab] = {Nu.a[0], Nu.a[1], Nu.a[2], Nu.a[3], Nv.a[0], Nv.a[1], Nv.a[2], Nv.a[3],
-                         D.a[0],  D.a[1],  D.a[2],  D.a[3],  C.a[0],  C.a[1],  C.a[2],  C.a[3], K, 0.0, 0.0, 0.0};
     for (int i = 0; i < kTab; i++) {
         td[o + i] = vals[i];
         tf[o + i] = (float)vals[i];
@@ -465,6 +479,362 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
     }
 }
 
+// ---------------------------------------------------------------- TMA-staged column kernel
+//
+// Geometries whose u coordinate and cone denominators do not depend on z
+// (Nu.z = D.z = C.z = 0 in every projection's table: circular orbits with the
+// rotation axis parallel to the detector columns, laminography tilted about x,
+// parallel beam) give each z-column of voxels one u, one weight and a v affine
+// in z per projection.  A CTA owns 32 x 8 columns of ZT voxels.  Per projection
+// the detector window its samples reach (bw x bh texels, bw a multiple of 4,
+// from the host's plan) is staged by one TMA copy into an S-stage ring of PB
+// projections per stage (warp 0 finds the windows, one lane per projection;
+// each warp releases a stage through an mbarrier, so warps drift up to S - 1
+// stages apart instead of meeting at a CTA barrier per stage).  Samples are
+// interpolated from shared memory with exact FP32 weights (floor and fraction
+// by the round-down 1.5 * 2^23 trick, v' = v - 1/2 one affine function of z per
+// column).  TMA's zero fill outside the detector is the reference's CLAMP
+// addressing.  A projection whose window for the tile exceeds the staged box
+// (where the plan underestimated it) is sampled from global memory instead.
+
+struct GBPColArgs {
+    const float *proj;    // [n][H][W]
+    const float *tab;     // [n][kTab] FP32 tables
+    const double *zvals;  // z value of each slice
+    uint32_t W, H, n_proj, nx, ny, nz, burst;
+    uint32_t bw, bh, slot_floats;  // staged window (texels, rows) and its shared-memory stride (floats)
+    float norm;
+    float *vol;
+    int *err;
+};
+
+template <int PB, int S>
+struct GBPColSmem {
+    float *data;     // [S][PB][slot_floats] staged windows
+    float4 *tab;     // [S][PB][kTab / 4] tables of the staged projections
+    int2 *org;       // [S][PB] window origin (u0, v0) in texels
+    uint64_t *full;  // [S] mbarriers: the stage's copies have landed
+    uint64_t *empty; // [S] mbarriers: all 8 warps are done with the stage
+    static size_t bytes(uint32_t slot_floats)
+    {
+        return (size_t)S * PB * slot_floats * 4 + (size_t)S * PB * kTab * 4 + (size_t)S * PB * 8 + (size_t)S * 16 + 128;
+    }
+    __device__ __forceinline__ GBPColSmem(unsigned char *dyn, uint32_t slot_floats)
+    {
+        unsigned char *raw = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~(uintptr_t)127);
+        data = reinterpret_cast<float *>(raw);
+        tab = reinterpret_cast<float4 *>(data + (size_t)S * PB * slot_floats);
+        org = reinterpret_cast<int2 *>(tab + S * PB * (kTab / 4));
+        full = reinterpret_cast<uint64_t *>(org + S * PB);
+        empty = full + S;
+    }
+};
+
+template <bool CONE, int ZT, int PB, int S>
+__global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUtensorMap map, const GBPColArgs c)
+{
+    static_assert(PB <= 32 && kTab % 4 == 0, "one producer lane per projection of a stage");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    const GBPColSmem<PB, S> sm(smem_dyn, c.slot_floats);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8, z0 = blockIdx.z * ZT;
+    // a warp covers 16 x 2 columns: its samples of one row then span fewer than 32 banks
+    const int ix = x0 + (warp & 1) * 16 + (lane & 15), iy = y0 + (warp >> 1) * 2 + (lane >> 4);
+    const float fx = (float)ix, fy = (float)iy;
+    float zv[ZT];
+#pragma unroll
+    for (int k = 0; k < ZT; k++) zv[k] = (float)c.zvals[min(z0 + k, (int)c.nz - 1)];
+    const float zlo = zv[0], zhi = zv[ZT - 1];
+    if (tid == 0) {
+        for (int q = 0; q < S; q++) {
+            mbar_init(&sm.full[q], 1);
+            mbar_init(&sm.empty[q], 8);
+        }
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    const int n = (int)c.n_proj, nblk = (n + PB - 1) / PB;
+    // Producer, all lanes of warp 0: lane q stages projection blk * PB + q once every warp has
+    // released the slot's previous stage.  Returns false if that wait gave up.
+    auto issue = [&](int blk) {
+        const int slot = blk % S, p = blk * PB + lane;
+        const int nval = min(PB, n - blk * PB);
+        if (blk >= S && !mbar_wait_bounded(&sm.empty[slot], (uint32_t)(blk / S - 1) & 1u, kWaitLimitNs)) return false;
+        int u0 = 0, v0 = 0;
+        if (lane < nval) {
+            const float4 *tr = reinterpret_cast<const float4 *>(c.tab + (size_t)p * kTab);
+            float t[kTab];
+#pragma unroll
+            for (int r = 0; r < kTab / 4; r++) {
+                const float4 w = __ldg(tr + r);
+                sm.tab[(slot * PB + lane) * (kTab / 4) + r] = w;
+                t[4 * r] = w.x;
+                t[4 * r + 1] = w.y;
+                t[4 * r + 2] = w.z;
+                t[4 * r + 3] = w.w;
+            }
+            // the extremes of a projective (or affine) map over the tile's box are at its corners
+            // (a cone denominator that changes sign inside the box has no such bound: not staged)
+            float umin = FLT_MAX, vmin = FLT_MAX, umax = -FLT_MAX, vmax = -FLT_MAX, dmin = 1.0f, dmax = 1.0f;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float cx = (float)(x0 + (i & 1) * 31), cy = (float)(y0 + (i >> 1) * 7);
+                const float uxy = fmaf(t[0], cx, fmaf(t[1], cy, t[3])), vxy = fmaf(t[4], cx, fmaf(t[5], cy, t[7]));
+                const float d = CONE ? fmaf(t[8], cx, fmaf(t[9], cy, t[11])) : 1.0f;
+                dmin = i ? fminf(dmin, d) : d;
+                dmax = i ? fmaxf(dmax, d) : d;
+                const float inv = 1.0f / d;
+                const float va = fmaf(t[6], zlo, vxy) * inv, vb = fmaf(t[6], zhi, vxy) * inv;
+                umin = fminf(umin, uxy * inv);
+                umax = fmaxf(umax, uxy * inv);
+                vmin = fminf(vmin, fminf(va, vb));
+                vmax = fmaxf(vmax, fmaxf(va, vb));
+            }
+            // left / upper tap = floor(x - 0.5) (rint(x) - 1 in the samples), one guard texel on
+            // each side for the samples' approximate reciprocals; x origin on a 16-byte boundary.
+            // A window larger than the staged box (or a degenerate one) sends the projection's
+            // samples of this tile to global memory.
+            const bool finite = fabsf(umin) < 4.0e6f && fabsf(umax) < 4.0e6f && fabsf(vmin) < 4.0e6f &&
+                                fabsf(vmax) < 4.0e6f && (dmin > 0.0f || dmax < 0.0f);
+            if (finite) {
+                u0 = ((int)floorf(umin - 0.5f) - 1) & ~3;
+                v0 = (int)floorf(vmin - 0.5f) - 1;
+            }
+            const bool fits = finite && (int)floorf(umax - 0.5f) + 2 - u0 <= (int)c.bw - 1 &&
+                              (int)floorf(vmax - 0.5f) + 2 - v0 <= (int)c.bh - 1;
+            sm.org[slot * PB + lane] = make_int2(fits ? u0 : INT_MIN, v0);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&sm.full[slot], (uint32_t)nval * c.bw * c.bh * 4u);
+        __syncwarp();
+        if (lane < nval) tma_load_3d(sm.data + (size_t)(slot * PB + lane) * c.slot_floats, &map, &sm.full[slot], u0, v0, p);
+        return true;
+    };
+    if (tid < 32)
+        for (int b = 0; b < S - 1 && b < nblk; b++) issue(b);
+
+    const float M1 = 12582911.0f;  // 1.5 * 2^23 - 1: (x + M1) - M1 = rint(x) for |x| < 2^22
+    const int M1b = __float_as_int(M1);
+    const float M = 12582912.0f;  // 1.5 * 2^23: x + M rounded down = floor(x) + M for |x| < 2^22
+    const int Mb = __float_as_int(M);
+    const float Wf = (float)c.W + 2.0f, Hf = (float)c.H + 2.0f;
+    const int bw = (int)c.bw;
+    float acc[ZT], bsum[ZT];
+#pragma unroll
+    for (int k = 0; k < ZT; k++) acc[k] = bsum[k] = 0.f;
+    uint32_t in_burst = 0;
+    bool aborted = false;
+    for (int blk = 0; blk < nblk; blk++) {
+        // the warps run up to S - 1 stages apart: no CTA-wide barrier per stage
+        if (tid < 32 && blk + S - 1 < nblk && !issue(blk + S - 1)) {
+            aborted = true;
+            break;
+        }
+        const int slot = blk % S;
+        const bool ok = mbar_wait_bounded(&sm.full[slot], (uint32_t)(blk / S) & 1u, kWaitLimitNs);
+        const int nval = min(PB, n - blk * PB);
+        if (ok) {
+            for (int q = 0; q < nval; q++) {
+                const int p = blk * PB + q;
+                float t[kTab];
+#pragma unroll
+                for (int r = 0; r < kTab / 4; r++)
+                    *reinterpret_cast<float4 *>(&t[4 * r]) = sm.tab[(slot * PB + q) * (kTab / 4) + r];
+                const int2 o = sm.org[slot * PB + q];
+                const float *win = sm.data + (size_t)(slot * PB + q) * c.slot_floats;
+                const float uxy = fmaf(t[0], fx, fmaf(t[1], fy, t[3]));
+                const float vxy = fmaf(t[4], fx, fmaf(t[5], fy, t[7]));
+                float inv = 1.0f, wgt = 1.0f;
+                if (CONE) {
+                    // approximate reciprocals (1 ulp), as the texture-gather path: u = Nu.X / D.X,
+                    // weight = (K / C.X)^2
+                    inv = rcp_approx(fmaf(t[8], fx, fmaf(t[9], fy, t[11])));
+                    const float cc = t[16] * rcp_approx(fmaf(t[12], fx, fmaf(t[13], fy, t[15])));
+                    wgt = cc * cc;
+                }
+                if (o.x != INT_MIN) {
+                    // the tile's footprints lie inside the staged window (one guard texel each side):
+                    // x' = x - 0.5 per axis, tap = floor(x') by adding 1.5 * 2^23 rounded down,
+                    // weight = x' - tap; v' is affine in z: v' = Av * z + Bv
+                    const float up = fmaf(uxy, inv, -0.5f);
+                    const float ru = __fadd_rd(up, M);
+                    const float a = up - (ru - M);
+                    const int iu = min(max(__float_as_int(ru) - Mb - o.x, 0), bw - 2);
+                    const float Av = t[6] * inv, Bv = fmaf(vxy, inv, -0.5f);
+                    const int vbase = Mb + o.y;
+                    const float *col = win + iu;
+#pragma unroll
+                    for (int k = 0; k < ZT; k++) {
+                        const float vp = fmaf(Av, zv[k], Bv);
+                        const float rv = __fadd_rd(vp, M);
+                        const float b = vp - (rv - M);
+                        const int iv = min(max(__float_as_int(rv) - vbase, 0), (int)c.bh - 2);
+                        const float *sp = col + iv * bw;
+                        const float t00 = sp[0], t10 = sp[1], t01 = sp[bw], t11 = sp[bw + 1];
+                        const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
+                        const float val = fmaf(b, bot - top, top);
+                        bsum[k] = CONE ? fmaf(val, wgt, bsum[k]) : bsum[k] + val;
+                    }
+                } else {
+                    // window not staged: the same footprints and weights from global memory
+                    const float *img = c.proj + (size_t)p * c.W * c.H;
+                    const float u = fminf(fmaxf(uxy * inv, -2.0f), Wf);
+                    const float ru = u + M1;
+                    const float a = (u + 0.5f) - (ru - M1);
+                    const int i0 = __float_as_int(ru) - M1b - 1;
+                    auto texel0 = [&](int i, int j) {
+                        return ((unsigned)i < c.W && (unsigned)j < c.H) ? __ldg(img + (size_t)j * c.W + i) : 0.f;
+                    };
+                    for (int k = 0; k < ZT; k++) {
+                        const float v = fminf(fmaxf(fmaf(t[6], zv[k], vxy) * inv, -2.0f), Hf);
+                        const float rv = v + M1;
+                        const float b = (v + 0.5f) - (rv - M1);
+                        const int j0 = __float_as_int(rv) - M1b - 1;
+                        const float t00 = texel0(i0, j0), t10 = texel0(i0 + 1, j0);
+                        const float t01 = texel0(i0, j0 + 1), t11 = texel0(i0 + 1, j0 + 1);
+                        const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
+                        const float val = fmaf(b, bot - top, top);
+                        bsum[k] = CONE ? fmaf(val, wgt, bsum[k]) : bsum[k] + val;
+                    }
+                }
+                if (++in_burst == c.burst || p + 1 == n) {
+#pragma unroll
+                    for (int k = 0; k < ZT; k++) {
+                        acc[k] = acc[k] + __fmul_rn(c.norm, bsum[k]);
+                        bsum[k] = 0.f;
+                    }
+                    in_burst = 0;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.empty[slot]);
+        if (!ok) {
+            aborted = true;
+            break;
+        }
+    }
+    // every loop above ends (all waits are bounded); a CTA that gave up lets its copies in
+    // flight land before it exits
+    if (__syncthreads_or(aborted)) {
+        if (tid == 0) {
+            atomicExch(c.err, kErrTmaTimeout);
+            for (int q = 0; q < S; q++)
+                for (int k = 0; k < 2; k++) mbar_wait_bounded(&sm.full[q], (uint32_t)k, kWaitLimitNs / 8);
+        }
+        return;
+    }
+    if (ix >= (int)c.nx || iy >= (int)c.ny) return;
+#pragma unroll
+    for (int k = 0; k < ZT; k++) {
+        if (z0 + k >= (int)c.nz) break;
+        c.vol[((size_t)(z0 + k) * c.ny + iy) * c.nx + ix] = acc[k];
+    }
+}
+
+// Staged-window plan of the column kernel for one geometry: whether every projection's table has
+// Nu.z = D.z = C.z = 0, and the window (bw x bh texels) that covers the 2x2 footprints of every
+// sample of a 32 x 8 x ZT voxel tile, from the tiles at 0, 1/4 .. 1 of the volume along each axis
+// (all projections), plus two texels of margin each way.
+struct GBPColPlan {
+    bool ok = false;
+    uint32_t bw = 0, bh = 0;
+};
+
+static constexpr int kColZT = 8;
+
+static GBPColPlan gbp_col_plan(const std::vector<double> &tabs, uint32_t n, bool cone, uint32_t nx, uint32_t ny,
+                               const std::vector<double> &zvals, uint32_t W, uint32_t H)
+{
+    GBPColPlan plan;
+    for (uint32_t p = 0; p < n; p++) {
+        const double *t = &tabs[(size_t)p * kTab];
+        if (t[2] != 0.0 || (cone && (t[10] != 0.0 || t[14] != 0.0))) return plan;
+    }
+    const uint32_t nz = (uint32_t)zvals.size();
+    const uint32_t tx = (nx + 31) / 32, ty = (ny + 7) / 8, tz = (nz + kColZT - 1) / kColZT;
+    auto picks = [](uint32_t m) {
+        std::vector<uint32_t> v;
+        for (int i = 0; i <= 4; i++) v.push_back((uint32_t)((uint64_t)(m - 1) * i / 4));
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        return v;
+    };
+    double wmax = 0, hmax = 0;
+    for (uint32_t bx : picks(tx))
+        for (uint32_t by : picks(ty))
+            for (uint32_t bz : picks(tz)) {
+                const double zl = zvals[bz * kColZT], zh = zvals[std::min(bz * kColZT + kColZT - 1, nz - 1)];
+                for (uint32_t p = 0; p < n; p++) {
+                    const double *t = &tabs[(size_t)p * kTab];
+                    double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+                    for (int i = 0; i < 4; i++) {
+                        const double cx = bx * 32.0 + (i & 1) * 31.0, cy = by * 8.0 + (i >> 1) * 7.0;
+                        const double inv = cone ? 1.0 / (t[8] * cx + t[9] * cy + t[11]) : 1.0;
+                        const double u = (t[0] * cx + t[1] * cy + t[3]) * inv;
+                        const double vxy = t[4] * cx + t[5] * cy + t[7];
+                        const double va = (vxy + t[6] * zl) * inv, vb = (vxy + t[6] * zh) * inv;
+                        umin = std::min(umin, u);
+                        umax = std::max(umax, u);
+                        vmin = std::min({vmin, va, vb});
+                        vmax = std::max({vmax, va, vb});
+                    }
+                    auto clampd = [](double x, double hi) { return std::min(std::max(x, -4.0), hi + 4.0); };
+                    umin = clampd(umin, W), umax = clampd(umax, W), vmin = clampd(vmin, H), vmax = clampd(vmax, H);
+                    const double u0 = std::floor(std::floor(umin - 0.5) - 1.0 - 3.0);  // worst case of the & ~3
+                    const double v0 = std::floor(vmin - 0.5) - 1.0;
+                    wmax = std::max(wmax, std::floor(umax - 0.5) + 2.0 - u0);
+                    hmax = std::max(hmax, std::floor(vmax - 0.5) + 2.0 - v0);
+                }
+            }
+    const double bw = std::ceil((wmax + 2.0) / 4.0) * 4.0, bh = hmax + 2.0;
+    if (!(bw >= 4 && bw <= 256 && bh >= 2 && bh <= 256)) return plan;
+    plan.ok = true;
+    plan.bw = (uint32_t)bw;
+    plan.bh = (uint32_t)bh;
+    return plan;
+}
+
+template <bool CONE, int PB, int S>
+static ufob_status launch_gbp_col_t(const GBPColArgs &c, cudaStream_t s)
+{
+    using Sm = GBPColSmem<PB, S>;
+    auto kern = k_gbp_col<CONE, kColZT, PB, S>;
+    static std::atomic<uint64_t> attr_devs{0};
+    const size_t smem = Sm::bytes(c.slot_floats);
+    UFOB_CUDA_TRY(smem_limit_per_device(kern, 227 * 1024, attr_devs));
+    CUtensorMap map;
+    UFOB_TRY(make_image_map(&map, c.proj, c.W, c.H, c.n_proj, c.W, (uint64_t)c.W * c.H, c.bw, c.bh));
+    dim3 grid((c.nx + 31) / 32, (c.ny + 7) / 8, (c.nz + kColZT - 1) / kColZT);
+    kern<<<grid, 256, smem, s>>>(map, c);
+    UFOB_CUDA_TRY(cudaGetLastError());
+    note_launch();
+    return UFOB_OK;
+}
+
+// Launches the column kernel with a ring that keeps two CTAs per SM; false when the window is too
+// large for that.
+static ufob_status launch_gbp_col(GBPColArgs c, bool cone, bool *launched, cudaStream_t s)
+{
+    *launched = false;
+    c.slot_floats = (c.bw * c.bh + 31) / 32 * 32;  // 128-byte aligned TMA destinations
+    constexpr size_t kBudget = 110 * 1024;           // two CTAs per SM
+    if (GBPColSmem<8, 3>::bytes(c.slot_floats) <= kBudget) {
+        *launched = true;
+        return cone ? launch_gbp_col_t<true, 8, 3>(c, s) : launch_gbp_col_t<false, 8, 3>(c, s);
+    }
+    if (GBPColSmem<8, 2>::bytes(c.slot_floats) <= kBudget) {
+        *launched = true;
+        return cone ? launch_gbp_col_t<true, 8, 2>(c, s) : launch_gbp_col_t<false, 8, 2>(c, s);
+    }
+    if (GBPColSmem<4, 3>::bytes(c.slot_floats) <= kBudget) {
+        *launched = true;
+        return cone ? launch_gbp_col_t<true, 4, 3>(c, s) : launch_gbp_col_t<false, 4, 3>(c, s);
+    }
+    return UFOB_OK;
+}
+
 template <bool CONE, typename CT, int RT, bool PARAMZ>
 static ufob_status launch_gbp_t(const GBPArgs &a, cudaStream_t s)
 {
@@ -559,6 +929,10 @@ struct ufob_gbp {
     int addressing_mode = AD_CLAMP;
     double gray_map_min = 0.0, gray_map_max = 0.0;
     int interpolation = 0;  // engine property: 0 exact FP32 weights, 1 the texture unit's linear filter
+    int staging = 1;        // engine property: 1 TMA-staged detector windows where the geometry allows, 0 never
+    // staging plan of the last geometry (host FP64 tables, window size), keyed by its inputs
+    std::vector<double> col_key;
+    GBPColPlan col_plan;
     // device state
     DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol, d_proj16;
     uint32_t pushed = 0, pw = 0, ph = 0;
@@ -743,6 +1117,10 @@ extern "C" ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *nam
         static const char *const kInterp[] = {"exact", "texture"};
         if ((i = lookup(value, kInterp, 2)) < 0) return fail(UFOB_ERR_INVALID, "unknown interpolation '%s'", value);
         g->interpolation = i;
+    } else if (name_is(name, "staging")) {  // engine property
+        static const char *const kStaging[] = {"texture", "auto"};
+        if ((i = lookup(value, kStaging, 2)) < 0) return fail(UFOB_ERR_INVALID, "unknown staging '%s'", value);
+        g->staging = i;
     } else {
         char *end = nullptr;
         double v = value ? strtod(value, &end) : 0.0;
@@ -912,6 +1290,42 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
                     : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
     }
     a.tab = g->d_tab_f.ptr;
+    if (g->compute_type == 0 && !g->interpolation && g->staging && g->result_type == RT_FLOAT &&
+        g->store_type == ST_FLOAT && paramz && a.addr == AD_CLAMP && W % 4 == 0 && !((uintptr_t)d_proj & 15)) {
+        // TMA-staged detector windows for geometries whose u does not depend on z; the plan (host
+        // FP64 tables, window size) is kept while the geometry stays the same
+        std::vector<double> key(table);
+        key.insert(key.end(), {(double)flags, x0, dxs, y0, dys, (double)nx, (double)ny, (double)W, (double)H});
+        key.insert(key.end(), zvals.begin(), zvals.end());
+        if (key != g->col_key) {
+            std::vector<double> tabs((size_t)n * kTab);
+            for (uint32_t p = 0; p < n; p++)
+                gbp_table_entry(&table[(size_t)p * GC_NCOLS], flags, x0, dxs, y0, dys, &tabs[(size_t)p * kTab]);
+            g->col_plan = gbp_col_plan(tabs, n, cone, nx, ny, zvals, W, H);
+            g->col_key.swap(key);
+        }
+        if (g->col_plan.ok) {
+            GBPColArgs c;
+            c.proj = d_proj;
+            c.tab = g->d_tab_f.as<float>();
+            c.zvals = a.zvals;
+            c.W = W;
+            c.H = H;
+            c.n_proj = n;
+            c.nx = nx;
+            c.ny = ny;
+            c.nz = nz;
+            c.burst = a.burst;
+            c.bw = g->col_plan.bw;
+            c.bh = g->col_plan.bh;
+            c.norm = (float)a.norm;
+            c.vol = static_cast<float *>(d_vol);
+            c.err = device_error_word();
+            bool launched = false;
+            UFOB_TRY(launch_gbp_col(c, cone, &launched, s));
+            if (launched) return UFOB_OK;
+        }
+    }
     if (g->compute_type == 2) {
         // FP16 samples: the gather unit returns 16-bit texels at twice the FP32 rate;
         // coordinates, weights and sums stay FP32
@@ -1215,6 +1629,38 @@ static ufob_status lamino_compute(ufob_lamino *l, const float *d_proj, uint32_t 
     a.vol = d_vol;
     a.tex = nullptr;
     a.hw_interp = 0;
+    if (paramz && a.addr == AD_CLAMP && W % 4 == 0 && !((uintptr_t)d_proj & 15)) {
+        // TMA-staged detector windows when u does not depend on z (no roll angle); the plan is
+        // kept while the tables stay the same
+        std::vector<double> key(tab.begin(), tab.end());
+        key.insert(key.end(), {(double)nx, (double)ny, (double)W, (double)H});
+        key.insert(key.end(), zvals.begin(), zvals.end());
+        if (key != g.col_key) {
+            g.col_plan = gbp_col_plan(std::vector<double>(tab.begin(), tab.end()), n, false, nx, ny, zvals, W, H);
+            g.col_key.swap(key);
+        }
+        if (g.col_plan.ok) {
+            GBPColArgs c;
+            c.proj = d_proj;
+            c.tab = g.d_tab_f.as<float>();
+            c.zvals = a.zvals;
+            c.W = W;
+            c.H = H;
+            c.n_proj = n;
+            c.nx = nx;
+            c.ny = ny;
+            c.nz = nz;
+            c.burst = a.burst;
+            c.bw = g.col_plan.bw;
+            c.bh = g.col_plan.bh;
+            c.norm = norm;
+            c.vol = d_vol;
+            c.err = device_error_word();
+            bool launched = false;
+            UFOB_TRY(launch_gbp_col(c, false, &launched, s));
+            if (launched) return UFOB_OK;
+        }
+    }
     if (gbp_textures(&g, d_proj, W, H, n, a.addr, s)) a.tex = g.d_tex.as<cudaTextureObject_t>();
     return launch_gbp_rt<false, float>(a, RT_FLOAT, paramz, s);
 }

@@ -297,6 +297,8 @@ ufob_status bp_batch_launch(const BatchBP *d_jobs, const uint2 *d_items, uint32_
                             SinoKind kind, bool kahan, int variant, cudaStream_t s);
 ufob_status make_sino_map(CUtensorMap *map, const void *base, uint32_t elems, uint32_t P, uint32_t nz,
                           uint32_t pitch, uint64_t slice_pitch, uint32_t box_x, uint32_t box_z);
+ufob_status make_image_map(CUtensorMap *map, const void *base, uint32_t W, uint32_t H, uint32_t n, uint64_t pitch,
+                           uint64_t plane, uint32_t box_w, uint32_t box_h);
 ufob_status bp_nearest_launch(const BPGeometry &g, const float *d_sino, uint32_t pitch, uint64_t slice_pitch,
                               float *d_out, cudaStream_t stream);
 

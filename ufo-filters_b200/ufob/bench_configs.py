@@ -9,7 +9,7 @@
 
 * general backprojection: 1024 projections of 1024^2 over 360 degrees into a
   512^3 volume, for the cone geometry (source 800 px before the axis, detector
-  200 px behind it), laminography (axis tilted by 30 degrees about x,
+  200 px behind it; both scale with --detector), laminography (axis tilted by 30 degrees about x,
   `axis-angle-x` = pi/6, 0 = tomography) and the parallel-beam case through the
   same task; inputs are uniform random projections (throughput does not depend
   on the values).  Each with exact FP32 interpolation weights (the default) and
@@ -62,18 +62,23 @@ def _timeit(fn, reps):
 
 
 def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "texture"),
-              computes=("float", "half")):
+              computes=("float", "half"), stagings=("auto",), geometries=None):
     import torch
     from . import GeneralBackprojectTask
     proj = torch.rand(n_proj, det, det, device="cuda")
-    geoms = {"cone": {"source-position-y": -800.0, "detector-position-y": 200.0},
+    # cone distances scale with the detector (800 / 200 px at 1024 px)
+    geoms = {"cone": {"source-position-y": -800.0 * det / 1024, "detector-position-y": 200.0 * det / 1024},
              "lamino_30deg": {"axis-angle-x": math.pi / 6},
              "parallel": {}}
+    if geometries:
+        geoms = {k: v for k, v in geoms.items() if k in geometries}
     out = []
-    for (name, g), interp, ct in [(gi, ip, c) for c in computes for ip in interpolations for gi in geoms.items()]:
+    for (name, g), interp, ct, st in [(gi, ip, c, sg) for c in computes for ip in interpolations for sg in stagings
+                                      for gi in geoms.items()]:
         t = GeneralBackprojectTask(num_projections=n_proj)
         t.set_property("interpolation", interp)
         t.set_property("compute-type", ct)
+        t.set_property("staging", st)
         t.set_property("center-position-x", det / 2.0)
         t.set_property("center-position-z", det / 2.0)
         half = vol / 2.0
@@ -86,7 +91,7 @@ def bench_gbp(reps=2, n_proj=1024, det=1024, vol=512, interpolations=("exact", "
         ms = _timeit(lambda: t.process(proj, out=v), reps)
         upd = float(vol) ** 3 * n_proj
         out.append({"workload": "general-backproject %s, %d projections of %d^2 -> %d^3" % (name, n_proj, det, vol),
-                    "interpolation": interp, "compute_type": ct, "ms": round(ms, 2),
+                    "interpolation": interp, "compute_type": ct, "staging": st, "ms": round(ms, 2),
                     "gups": round(upd / ms / 1e6, 1)})
     return out
 
@@ -226,6 +231,10 @@ def main(argv=None):
                     help="compute-type(s) of the general backprojection")
     ap.add_argument("--gbp-interp", choices=["exact", "texture", "both"], default="both",
                     help="interpolation mode(s) of the general backprojection")
+    ap.add_argument("--gbp-staging", choices=["auto", "texture", "both"], default="auto",
+                    help="staging of the general backprojection: TMA-staged windows where the geometry "
+                         "allows (auto) or texture gathers")
+    ap.add_argument("--gbp-geometries", default="", help="comma-separated subset of cone,lamino_30deg,parallel")
     args = ap.parse_args(argv)
     from . import device_status
     rows = []
@@ -233,7 +242,9 @@ def main(argv=None):
     if args.gbp or not only:
         computes = ("float", "half") if args.gbp_compute == "both" else (args.gbp_compute,)
         interps = ("exact", "texture") if args.gbp_interp == "both" else (args.gbp_interp,)
-        rows += bench_gbp(args.reps, args.projections, args.detector, args.volume, interps, computes)
+        stagings = ("auto", "texture") if args.gbp_staging == "both" else (args.gbp_staging,)
+        geoms = [g for g in args.gbp_geometries.split(",") if g] or None
+        rows += bench_gbp(args.reps, args.projections, args.detector, args.volume, interps, computes, stagings, geoms)
     if args.batch or not only:
         rows += bench_batch()
     if args.pre or not only:
