@@ -379,15 +379,22 @@ def run_configs(ufob, torch, dev, seed):
     net = SparseViewNet.pretrained()
     seeds = list(range(1_000_000, 1_000_064))
     imgs = maker.phantoms(seeds)
-    x = maker.fbp_sparse.process(maker.sinograms(imgs, maker.sparse))
+    s_sparse = maker.sinograms(imgs, maker.sparse)
+    x = maker.fbp_sparse.process(s_sparse)
+    x16 = ufob.FBP(storage=ufob.F16).process(s_sparse)
     y = maker.fbp_dense.process(maker.sinograms(imgs, maker.dense))
+    times = [time_paths(net, maker, B=b) for b in (64, 128, 256)]
     table["c4_learned_sparse_view"] = {
         "workload": "90-angle 512 px FBP + 4-level CNN (32/64/128/256 ch, BF16 tensor cores) vs 1800-angle FBP, "
                     "shipped weights, 64 held-out phantoms (seeds 1e6..)",
         "plain_fbp90_rel_l2_vs_1800": round(float(rel_l2(x, y).mean()), 5),
         "cnn_rel_l2_vs_1800": round(float(rel_l2(net.forward(x), y).mean()), 5),
-        "time_per_slice": [time_paths(net, maker, B=b) for b in (64, 128, 256)]}
-    del imgs, x, y, net, maker
+        "cnn_on_fp16_fbp90_rel_l2_vs_1800": round(float(rel_l2(net.forward(x16), y).mean()), 5),
+        # the engine's learned path (FP16-storage 90-angle FBP + network) against the plain FP32
+        # dense FBP, per batch size; the per-form ratios are under time_per_slice
+        "learned_path_speedup_vs_plain_dense": {str(t["batch"]): t["fp16_learned_vs_plain_dense"] for t in times},
+        "time_per_slice": times}
+    del imgs, s_sparse, x, x16, y, net, maker
     torch.cuda.empty_cache()
     return table, checks
 

@@ -1146,13 +1146,28 @@ ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind k
     }
 }
 
-// out[i] = sum over the angle groups of part[k][i], in group order
+// out[i] = sum over the angle groups of part[k][i], in group order; four pixels per thread
+// (plane % 4 == 0, 16-byte aligned buffers) or one
+template <int V>
 __global__ void k_sum_groups(const float *__restrict__ part, uint64_t plane, uint32_t groups, float *__restrict__ out)
 {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < plane; i += (uint64_t)gridDim.x * blockDim.x) {
-        float v = part[i];
-        for (uint32_t k = 1; k < groups; k++) v += part[(uint64_t)k * plane + i];
-        out[i] = v;
+    const uint64_t n = plane / V;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        if (V == 4) {
+            float4 v = reinterpret_cast<const float4 *>(part)[i];
+            for (uint32_t k = 1; k < groups; k++) {
+                const float4 w = reinterpret_cast<const float4 *>(part + (uint64_t)k * plane)[i];
+                v.x += w.x;
+                v.y += w.y;
+                v.z += w.z;
+                v.w += w.w;
+            }
+            reinterpret_cast<float4 *>(out)[i] = v;
+        } else {
+            float v = part[i];
+            for (uint32_t k = 1; k < groups; k++) v += part[(uint64_t)k * plane + i];
+            out[i] = v;
+        }
     }
 }
 
@@ -1184,8 +1199,13 @@ ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, Sino
                                                                              stream, gg.P);
     UFOB_TRY(st);
     const uint64_t plane = (uint64_t)g.roi_w * g.roi_h;
-    const uint32_t grid = (uint32_t)std::min<uint64_t>((plane + 255) / 256, (uint64_t)num_sms() * 8);
-    k_sum_groups<<<grid, 256, 0, stream>>>(d_part, plane, groups, d_out);
+    const bool vec = !(plane & 3) && !(((uintptr_t)d_part | (uintptr_t)d_out) & 15);
+    const uint64_t items = vec ? plane / 4 : plane;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((items + 255) / 256, (uint64_t)num_sms() * 8);
+    if (vec)
+        k_sum_groups<4><<<grid, 256, 0, stream>>>(d_part, plane, groups, d_out);
+    else
+        k_sum_groups<1><<<grid, 256, 0, stream>>>(d_part, plane, groups, d_out);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
