@@ -154,6 +154,9 @@ typedef struct {
     int half_sums;            /* F16 QUADS sinograms only: 0 (default) every product accumulated in
                                  FP32; 1 interpolation and sums over blocks of 8 angles in packed
                                  FP16, block sums accumulated in FP32 (faster, larger error) */
+    int angle_groups;         /* one F32/pair sinogram: 0 (default) automatic, 1 one launch, 2/4/8
+                                 equal angle groups backprojected as slices of one launch whose
+                                 partial images are summed in group order */
 } ufob_bp_props;
 
 typedef struct ufob_backproject ufob_backproject;

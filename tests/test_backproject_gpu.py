@@ -136,28 +136,15 @@ def test_pairs_single_slice_tiles(cuda, dtype, tol, tile, kahan):
 
 
 @pytest.mark.parametrize("dtype,tol", [(ufob.F32, 3e-5), (ufob.F16, 1e-3), (ufob.BF16, 8e-3)])
-def test_single_sinogram_angle_groups(cuda, dtype, tol):
-    """A small sinogram with 1536 angles is backprojected as equal angle groups whose partial
-    images are summed (compensated sums for the 16-bit forms); same result as the oracle and,
-    within round-off, as the unsplit kernel (an explicit tile).  FP32 bound: 1536 angles of a
-    noise sinogram, whose slice is small against its terms."""
+@pytest.mark.parametrize("groups,tile", [(2, 10), (4, 8), (8, 11), (4, 9), (2, 0)])
+def test_single_sinogram_angle_groups(cuda, dtype, tol, groups, tile):
+    """A sinogram with 1536 angles backprojected as equal angle groups (the slices of one launch,
+    partial images summed in group order; compensated sums for the 16-bit forms), for every
+    single-slice tile shape: same result as the oracle and, within round-off, as one launch of the
+    same tile.  FP32 bound: 1536 angles of a noise sinogram, whose slice is small against its
+    terms."""
     rng = np.random.default_rng(21)
     W, P = 512, 1536
-    # the engine's choice (capi.cu split_groups): 16 x 6 tiles of 32x96 pixels per group, split
-    # into 2, 4 or 8 groups when that lowers the busiest SM's share over the average by > 0.05
-    sms = torch.cuda.get_device_properties(0).multi_processor_count
-    tiles = ((W + 31) // 32) * ((W + 95) // 96)
-
-    def imbalance(k):
-        per_sm = tiles * k / sms
-        return math.ceil(per_sm) / per_sm
-    groups, best = 1, imbalance(1)
-    for k in (2, 4, 8):
-        if P % k or P // k < 32:
-            break
-        if imbalance(k) < best - 0.05:
-            groups, best = k, imbalance(k)
-    assert groups > 1, "the case must exercise the angle-group split on this GPU (%d SMs)" % sms
     raw = rng.standard_normal((P, W)).astype(np.float32)
     f = ufob.FilterTask()
     ref = oracle.backproject(oracle.fft_filter_ifft(raw).astype(np.float32))
@@ -168,11 +155,26 @@ def test_single_sinogram_angle_groups(cuda, dtype, tol):
         kw = dict(dtype=dtype, layout=ufob.PAIRS, width=W)
     torch.cuda.synchronize()
     n0 = ufob.launch_count()
-    got = ufob.BackprojectTask().process(src, **kw).cpu().numpy()
+    got = ufob.BackprojectTask(tile=tile, angle_groups=groups).process(src, **kw).cpu().numpy()
     n1 = ufob.launch_count()
-    unsplit = ufob.BackprojectTask(tile=8).process(src, **kw).cpu().numpy()
+    unsplit = ufob.BackprojectTask(tile=tile, angle_groups=1).process(src, **kw).cpu().numpy()
     n2 = ufob.launch_count()
     # the split run adds exactly one launch: the ordered sum of the partial images
     assert (n1 - n0) == (n2 - n1) + 1
     assert oracle.rel_l2(got, ref) < tol
     assert oracle.rel_l2(got, unsplit) < 1e-5
+
+
+def test_automatic_plan_matches_oracle(cuda):
+    """The automatic tile / angle-group plan of one sinogram at several sizes (whatever it picks)
+    against the oracle, and an impossible pinned split is refused."""
+    rng = np.random.default_rng(22)
+    for W, P in [(512, 512), (256, 256), (1024, 1024), (300, 96), (128, 40)]:
+        raw = rng.standard_normal((P, W)).astype(np.float32)
+        filt = ufob.FilterTask(size_x=1 << (W - 1).bit_length(), crop_width=W).process(torch.from_numpy(raw).cuda())
+        got = ufob.BackprojectTask().process(filt).cpu().numpy()
+        ref = oracle.backproject(oracle.fft_filter_ifft(raw, size_x=1 << (W - 1).bit_length(),
+                                                        crop_width=W).astype(np.float32))
+        assert oracle.rel_l2(got, ref) < 3e-5, (W, P)
+    with pytest.raises(ufob.UfobError):
+        ufob.BackprojectTask(angle_groups=8).process(filt)  # 40 rows: groups of 5

@@ -941,10 +941,16 @@ static ufob_status launch_linear(const BPGeometry &g, const void *d_sino, uint32
 
 template <int KIND, bool KAHAN>
 static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_sino, uint32_t elems, uint32_t pitch,
-                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream)
+                                 uint64_t slice_pitch, float *d_out, cudaStream_t stream, uint32_t zstride = 0)
 {
     switch (tile) {
-    case 0: return launch_linear<32, 16, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
+    // single-slice shapes (ZT = 1), also the slices of an angle-group split (zstride: table rows
+    // per group)
+    case 0: return launch_linear<32, 16, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream, zstride);
+    case 8: return launch_linear<32, 96, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream, zstride);
+    case 9: return launch_linear<32, 32, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream, zstride);
+    case 10: return launch_linear<32, 64, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream, zstride);
+    case 11: return launch_linear<32, 128, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream, zstride);
     case 1: return launch_linear<32, 32, 2, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 2: return launch_linear<32, 32, 4, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 3: return launch_linear<32, 16, 4, 16, 4, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
@@ -952,8 +958,6 @@ static ufob_status dispatch_tile(int tile, const BPGeometry &g, const void *d_si
     case 5: return launch_linear<32, 16, 8, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 6: return launch_linear<32, 32, 8, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     case 7: return launch_linear<32, 16, 4, 32, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
-    case 8: return launch_linear<32, 96, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
-    case 9: return launch_linear<32, 32, 1, 16, 3, KIND, KAHAN>(g, d_sino, elems, pitch, slice_pitch, d_out, stream);
     default: return fail(UFOB_ERR_INVALID, "backproject: unknown tile id %d", tile);
     }
 }
@@ -1172,10 +1176,14 @@ __global__ void k_sum_groups(const float *__restrict__ part, uint64_t plane, uin
 }
 
 ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
-                                   uint32_t groups, float *d_part, float *d_out, bool kahan, cudaStream_t stream)
+                                   uint32_t groups, int tile, float *d_part, float *d_out, bool kahan,
+                                   cudaStream_t stream)
 {
     if (!groups || g.nz != 1 || g.P % groups)
         return fail(UFOB_ERR_INVALID, "backproject: %u angle groups for %u rows of one sinogram", groups, g.P);
+    if (!(tile == 0 || tile == 8 || tile == 9 || tile == 10 || tile == 11))
+        return fail(UFOB_ERR_INVALID, "backproject: angle groups need a single-slice tile (0, 8, 9, 10, 11), not %d",
+                    tile);
     if (((uintptr_t)d_sino & 15) || (pitch & 3))
         return fail(UFOB_ERR_INVALID, "backproject: sinogram base/pitches must be 16-byte aligned");
     BPGeometry gg = g;
@@ -1185,18 +1193,14 @@ ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, Sino
     const uint64_t sp = (uint64_t)gg.P * pitch;
     ufob_status st;
     if (kind == SINO_F32)
-        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_F32, true>(gg, d_sino, elems, pitch, sp, d_part, stream, gg.P)
-                   : launch_linear<32, 96, 1, 16, 3, SINO_F32, false>(gg, d_sino, elems, pitch, sp, d_part, stream, gg.P);
+        st = kahan ? dispatch_tile<SINO_F32, true>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P)
+                   : dispatch_tile<SINO_F32, false>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P);
     else if (kind == SINO_F16_PAIRS)
-        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_F16_PAIRS, true>(gg, d_sino, elems, pitch, sp, d_part, stream,
-                                                                           gg.P)
-                   : launch_linear<32, 96, 1, 16, 3, SINO_F16_PAIRS, false>(gg, d_sino, elems, pitch, sp, d_part, stream,
-                                                                            gg.P);
+        st = kahan ? dispatch_tile<SINO_F16_PAIRS, true>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P)
+                   : dispatch_tile<SINO_F16_PAIRS, false>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P);
     else
-        st = kahan ? launch_linear<32, 96, 1, 16, 3, SINO_BF16_PAIRS, true>(gg, d_sino, elems, pitch, sp, d_part, stream,
-                                                                            gg.P)
-                   : launch_linear<32, 96, 1, 16, 3, SINO_BF16_PAIRS, false>(gg, d_sino, elems, pitch, sp, d_part,
-                                                                             stream, gg.P);
+        st = kahan ? dispatch_tile<SINO_BF16_PAIRS, true>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P)
+                   : dispatch_tile<SINO_BF16_PAIRS, false>(tile, gg, d_sino, elems, pitch, sp, d_part, stream, gg.P);
     UFOB_TRY(st);
     const uint64_t plane = (uint64_t)g.roi_w * g.roi_h;
     const bool vec = !(plane & 3) && !(((uintptr_t)d_part | (uintptr_t)d_out) & 15);

@@ -374,7 +374,7 @@ struct ufob_backproject {
     ufob_bp_props props;
     DevBuf sincos;
     DevBuf aligned;  // copy of a sinogram whose pitch is not TMA-compatible
-    DevBuf partial;  // per-angle-group images of one small sinogram (split_groups)
+    DevBuf partial;  // per-angle-group images of one small sinogram (split_plan)
     // cache key of the sin/cos table
     uint32_t key_P = 0, key_nproj = 0, key_offset = 0;
     double key_step = 0, key_aoff = 0;
@@ -397,6 +397,7 @@ void ufob_bp_props_init(ufob_bp_props *p)
     p->compensated = -1;
     p->tile = -1;
     p->half_sums = 0;
+    p->angle_groups = 0;
 }
 
 static ufob_status validate_bp_props(const ufob_bp_props *p)
@@ -439,6 +440,12 @@ ufob_status ufob_backproject_set_property(ufob_backproject *bp, const char *name
     else if (prop_is(name, "compensated")) p.compensated = (int)v;
     else if (prop_is(name, "tile")) p.tile = (int)v;
     else if (prop_is(name, "half-sums")) p.half_sums = (int)v;
+    else if (prop_is(name, "angle-groups")) {
+        const int k = (int)v;
+        if (!(k == 0 || k == 1 || k == 2 || k == 4 || k == 8) || (double)k != v)
+            return fail(UFOB_ERR_INVALID, "angle-groups must be 0 (automatic), 1, 2, 4 or 8");
+        p.angle_groups = k;
+    }
     else return fail(UFOB_ERR_INVALID, "backproject: no property named '%s'", name ? name : "(null)");
     if ((prop_is(name, "num-projections") || prop_is(name, "offset") || prop_is(name, "roi-x") ||
          prop_is(name, "roi-y") || prop_is(name, "roi-width") || prop_is(name, "roi-height")) && v < 0)
@@ -533,22 +540,44 @@ static bool want_kahan(const ufob_bp_props &p, SinoKind kind, uint32_t P)
 // A single sinogram is split into 2, 4 or 8 equal angle groups (at least 32 angles each) whose
 // partial images are summed, when that spreads its 32x96 tiles more evenly over the SMs: the
 // busiest SM's share of tiles over the average one drops by more than 5%; 1 = no split.
-static uint32_t split_groups(const BPGeometry &g)
+// Launch plan of one sinogram (nz == 1): tile shape (single-slice ids: 32 x 16, 32, 64, 96, 128
+// pixels) and angle groups (1, 2, 4, 8; each group >= 32 rows).  A plan is scored by the time of
+// its busiest SM: CTAs (tiles x groups, a partial tile costing a full one) spread evenly, each SM
+// running its share at the tile's measured update rate (half of it with a single CTA per SM,
+// whose 8 warps do not fill the SM), plus the ordered sum of the partial images at HBM speed.
+// Ties keep the earlier candidate.  A caller's tile or group count pins that part of the plan.
+struct SplitPlan {
+    int tile;
+    uint32_t groups;
+};
+
+static SplitPlan split_plan(const BPGeometry &g, int fixed_tile, int fixed_groups)
 {
-    if (g.nz != 1) return 1;
-    const double tiles = (double)((g.roi_w + 31) / 32) * (double)((g.roi_h + 95) / 96), sms = (double)num_sms();
-    auto imbalance = [&](uint32_t k) {
-        const double per_sm = tiles * k / sms;
-        return std::ceil(per_sm) / per_sm;
+    // per-SM update rate of each single-slice tile relative to 32 x 96, measured on B200 from one
+    // 2048^2 sinogram of 1500 angles (32 x 96: 14.0 G updates/s per SM)
+    struct Cand {
+        int tile;
+        uint32_t rows;
+        double rate;
     };
-    uint32_t best = 1;
-    double best_im = imbalance(1);
-    for (uint32_t k = 2; k <= 8; k *= 2) {
-        if (g.P % k || g.P / k < 32) break;
-        const double im = imbalance(k);
-        if (im < best_im - 0.05) {
-            best = k;
-            best_im = im;
+    static const Cand kCands[] = {{8, 96, 1.0}, {11, 128, 0.979}, {10, 64, 0.878}, {9, 32, 0.779}, {0, 16, 0.608}};
+    const double sms = (double)num_sms(), sm_rate = 14.03e9;
+    SplitPlan best{fixed_tile, 1};
+    if (g.nz != 1) return best;
+    double best_t = 1e300;
+    for (const Cand &c : kCands) {
+        if (fixed_tile >= 0 && c.tile != fixed_tile) continue;
+        for (uint32_t k = 1; k <= 8; k *= 2) {
+            if (fixed_groups > 0 && k != (uint32_t)fixed_groups) continue;
+            if (k > 1 && (g.P % k || g.P / k < 32)) continue;
+            const double ctas = (double)((g.roi_w + 31) / 32) * (double)((g.roi_h + c.rows - 1) / c.rows) * k;
+            const double per_sm = std::ceil(ctas / sms);
+            double t = per_sm * 32.0 * c.rows * (double)(g.P / k) / (sm_rate * c.rate * std::min(1.0, per_sm / 2.0));
+            if (k > 1) t += (k + 1) * 4.0 * g.roi_w * g.roi_h / 6.0e12 + 3.0e-6;
+            if (t < best_t * (1.0 - 1e-9)) {
+                best_t = t;
+                best = SplitPlan{c.tile, k};
+            }
         }
     }
     return best;
@@ -605,12 +634,18 @@ extern "C" ufob_status ufob_backproject_run(ufob_backproject *bp, const void *d_
         slice_pitch = (uint64_t)ap * height;
     }
     const bool kahan = want_kahan(bp->props, kind, height);
-    const uint32_t groups = bp->props.tile < 0 ? split_groups(g) : 1;
-    if (groups > 1) {
-        UFOB_TRY(bp->partial.ensure((size_t)groups * g.roi_w * g.roi_h * sizeof(float)));
-        return bp_linear_split_launch(g, src, kind, pitch, groups, bp->partial.as<float>(), d_out, kahan, s);
+    const SplitPlan plan = split_plan(g, bp->props.tile, bp->props.angle_groups);
+    if (bp->props.angle_groups > 1 && plan.groups != (uint32_t)bp->props.angle_groups)
+        return fail(UFOB_ERR_INVALID,
+                    "backproject: angle-groups %d needs one sinogram whose %u rows split into groups of >= 32 and a "
+                    "single-slice tile (0, 8, 9, 10, 11)",
+                    bp->props.angle_groups, height);
+    if (plan.groups > 1) {
+        UFOB_TRY(bp->partial.ensure((size_t)plan.groups * g.roi_w * g.roi_h * sizeof(float)));
+        return bp_linear_split_launch(g, src, kind, pitch, plan.groups, plan.tile, bp->partial.as<float>(), d_out,
+                                      kahan, s);
     }
-    return bp_linear_launch(g, src, kind, pitch, slice_pitch, d_out, kahan, bp->props.tile, s);
+    return bp_linear_launch(g, src, kind, pitch, slice_pitch, d_out, kahan, plan.tile, s);
 }
 
 extern "C" void ufob_backproject_destroy(ufob_backproject *bp) { delete bp; }
@@ -713,7 +748,7 @@ extern "C" ufob_status ufob_stacked_bp_set_property(ufob_stacked_bp *sb, const c
         sb->precision = (int)v;
         return UFOB_OK;
     }
-    if (prop_is(name, "mode") || prop_is(name, "tile") || prop_is(name, "half-sums"))
+    if (prop_is(name, "mode") || prop_is(name, "tile") || prop_is(name, "half-sums") || prop_is(name, "angle-groups"))
         return fail(UFOB_ERR_INVALID, "stacked-backproject: no property named '%s'", name);
     return ufob_backproject_set_property(sb->bp, name, v);
 }

@@ -246,7 +246,8 @@ ufob_status bp_linear_launch(const BPGeometry &g, const void *d_sino, SinoKind k
 // One sinogram split into `groups` angle groups of height / groups rows (tile 8, slice z = group
 // z), partial images summed into d_out; d_part holds groups x roi_h x roi_w floats.
 ufob_status bp_linear_split_launch(const BPGeometry &g, const void *d_sino, SinoKind kind, uint32_t pitch,
-                                   uint32_t groups, float *d_part, float *d_out, bool kahan, cudaStream_t stream);
+                                   uint32_t groups, int tile, float *d_part, float *d_out, bool kahan,
+                                   cudaStream_t stream);
 
 // Slice-quad FP16 form (four slices' tap pairs per 16-byte cell): filter stage
 // and backprojection.  acc: 0 FP32 accumulation of every product, 1 FP16 lerp

@@ -48,7 +48,7 @@ class BPProps(ctypes.Structure):
                 ("angle_step", ctypes.c_double), ("angle_offset", ctypes.c_double), ("mode", ctypes.c_int),
                 ("roi_x", ctypes.c_uint32), ("roi_y", ctypes.c_uint32), ("roi_width", ctypes.c_uint32),
                 ("roi_height", ctypes.c_uint32), ("compensated", ctypes.c_int), ("tile", ctypes.c_int),
-                ("half_sums", ctypes.c_int)]
+                ("half_sums", ctypes.c_int), ("angle_groups", ctypes.c_int)]
 
 
 class Job(ctypes.Structure):
