@@ -594,6 +594,13 @@ def main():
                 "gups_achieved_kernel": upd_per_launch / avg_launch_s / 1e9,
                 "gups_roofline": smem_gbs / gather_bytes,
                 "fp32_tflops_measured": fp32_tflops}
+    # independent cross-check of the measured peak: 128 bytes per SM per clock (one shared-memory
+    # wavefront) at the median SM clock sampled during the timed region
+    sm_mhz = chosen["clocks"].get("sm_mhz")
+    if sm_mhz:
+        nominal = torch.cuda.get_device_properties(dev).multi_processor_count * 128.0 * sm_mhz * 1e6 / 1e9
+        roofline["peak_nominal_gbs"] = nominal
+        roofline["frac_of_nominal"] = achieved / nominal
     hbm_peak = None
     try:
         hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
