@@ -117,6 +117,33 @@ ufob_status sincos_table_launch(double angle_offset, double step, uint32_t lut_o
 
 // ------------------------------------------------------------------ linear kernel
 
+// Shared-memory stride (32-bit words) between the staged boxes of consecutive angles of the
+// row kernel: 128-byte aligned for the TMA destination, and never a multiple of 512 bytes
+// (measured on B200: a 512-byte stride made the 32 x 96 single-slice kernel 10% slower; the
+// slice-quad kernel measured no such effect and keeps its plain 128-byte rounding).
+constexpr int box_stride(int words)
+{
+    return ((words + 31) / 32 * 32) % 128 == 0 ? (words + 31) / 32 * 32 + 32 : (words + 31) / 32 * 32;
+}
+
+// Smallest s with s * s >= v.
+constexpr int isqrt_ceil(int v)
+{
+    int r = 0;
+    while (r * r < v) ++r;
+    return r;
+}
+
+// Detector bins a TX x TY pixel tile reaches at any angle: its projected extent is at most the
+// diagonal sqrt((TX-1)^2 + (TY-1)^2), plus one for the floor of the lower end.
+template <int TX, int TY>
+constexpr int tile_span()
+{
+    return 1 + isqrt_ceil((TX - 1) * (TX - 1) + (TY - 1) * (TY - 1)) < (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1))
+               ? 1 + isqrt_ceil((TX - 1) * (TX - 1) + (TY - 1) * (TY - 1))
+               : (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
+}
+
 template <int TX, int TY, int ZT, int A, int S>
 struct BPShape {
     static constexpr int kThreads = 256;
@@ -125,10 +152,10 @@ struct BPShape {
     static_assert(kRY >= 1 && kRY * (kThreads / TX) == TY, "tile height");
     // window of detector elements reachable by the tile, plus interpolation tap,
     // one guard element on each side and 3 for the 16-byte TMA alignment
-    static constexpr int kSpan = (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
+    static constexpr int kSpan = tile_span<TX, TY>();
     static constexpr int kWin = ((kSpan + 2 + 2 + 3) + 3) / 4 * 4;
     // each angle's box lands at a 128-byte aligned shared address (TMA destination rule)
-    static constexpr int kAngleStride = (ZT * kWin + 31) / 32 * 32;
+    static constexpr int kAngleStride = box_stride(ZT * kWin);
     static constexpr int kStageElems = A * kAngleStride;
     static constexpr size_t kDataBytes = (size_t)S * kStageElems * 4;
     static constexpr size_t kWinOffset = kDataBytes;
@@ -612,7 +639,7 @@ struct BPQShape {
     static constexpr int kRY = TY / (kThreads / TX);
     static_assert(TX == 32 && ZT % 4 == 0, "one warp spans the tile width; whole slice groups");
     static_assert(kRY >= 1 && kRY * (kThreads / TX) == TY, "tile height");
-    static constexpr int kSpan = (int)(1.0 + 1.4143 * (TX > TY ? TX - 1 : TY - 1));
+    static constexpr int kSpan = tile_span<TX, TY>();
     static constexpr int kWin = (kSpan + 2 + 2 + 1) / 2 * 2;  // + tap + guard on each side
     static constexpr int kGroups = ZT / 4;
     static constexpr int kAngleStride = (kGroups * kWin * 4 + 31) / 32 * 32;  // words; 128-byte aligned boxes

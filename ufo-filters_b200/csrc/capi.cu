@@ -560,8 +560,8 @@ static SplitPlan split_plan(const BPGeometry &g, int fixed_tile, int fixed_group
         uint32_t rows;
         double rate;
     };
-    static const Cand kCands[] = {{8, 96, 1.0}, {11, 128, 0.979}, {10, 64, 0.878}, {9, 32, 0.779}, {0, 16, 0.608}};
-    const double sms = (double)num_sms(), sm_rate = 14.03e9;
+    static const Cand kCands[] = {{8, 96, 1.0}, {11, 128, 0.979}, {10, 64, 0.942}, {9, 32, 0.780}, {0, 16, 0.609}};
+    const double sms = (double)num_sms(), sm_rate = 14.01e9;
     SplitPlan best{fixed_tile, 1};
     if (g.nz != 1) return best;
     double best_t = 1e300;
