@@ -92,6 +92,13 @@ __device__ __forceinline__ bool bar_wait(uint64_t *b, uint32_t parity, volatile 
     }
 }
 
+// Programmatic dependent launch: the next kernel of the forward pass may be scheduled as soon as
+// every CTA of this one has started (launch_dependents); a kernel launched that way waits for its
+// predecessor, and hence for every earlier kernel of the stream, to complete and become visible
+// (wait) before it reads their outputs.  Both are no-ops without the launch attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void bar_arrive(uint64_t *b)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sa(b)) : "memory");
@@ -260,6 +267,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
     __shared__ float s_bias[256];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    pdl_launch_dependents();
     const int Cin = a.Cin, Cout = a.Cout;
     const int cgc = Cin < 64 ? Cin / 8 : 8;  // channel groups per K chunk
     const int nchunks = Cin / (cgc * 8);
@@ -326,6 +334,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
                         last_b[sb] = 0;
                     }
             }
+            pdl_wait();  // the activations are the previous kernels' outputs
             for (long long tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x) {
                 const long long q0 = tile * (long long)(MT * 128);
                 for (int kc = 0; kc < nchunks && ok; kc++) {
@@ -418,6 +427,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
         const uint32_t Hp = (uint32_t)a.gi.H + 2;
         const uint32_t img_rows = Hp * (uint32_t)Wp;
         const uint32_t rows = (uint32_t)a.gi.rows;
+        pdl_wait();  // skip tensors and the FBP image come from earlier kernels
         for (long long tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, it++) {
             const uint32_t ab = it & 1u;
             if (!bar_wait(&t_full[ab], (it >> 1) & 1u, abort_p)) {
@@ -592,6 +602,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
 // fbp [B][4H][4W] -> CG x0 (16 channels, two planes): channel 4*dy + dx = fbp[4y+dy][4x+dx] / s
 __global__ void k_cg_unshuffle(const float *__restrict__ fbp, bf16 *__restrict__ x0, CGGeom g, float inv_s)
 {
+    pdl_launch_dependents();
     const long long n = (long long)g.B * g.H * g.W;
     CG_LOOP(i, n) {
         const int x = (int)(i % g.W), y = (int)((i / g.W) % g.H);
@@ -622,6 +633,8 @@ __global__ void k_cg_unshuffle(const float *__restrict__ fbp, bf16 *__restrict__
 // 2x2 average pool between CG tensors (gi -> go = gi / 2), C/8 planes
 __global__ void k_cg_pool(const bf16 *__restrict__ in, bf16 *__restrict__ out, CGGeom gi, CGGeom go, int planes)
 {
+    pdl_launch_dependents();
+    pdl_wait();
     const long long n = (long long)planes * go.B * go.H * go.W;
     CG_LOOP(i, n) {
         const int x = (int)(i % go.W), y = (int)((i / go.W) % go.H);
@@ -794,7 +807,17 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
     }
     // one CTA per SM: the two accumulator buffers may take all 512 TMEM columns
     const long long grid = std::min<long long>(a.ntiles, num_sms());
-    kern<<<(unsigned)grid, kThreads, std::max<size_t>(smem, 116 * 1024), s>>>(a);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = std::max<size_t>(smem, 116 * 1024);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, a);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess)
         return fail(UFOB_ERR_CUDA, "cnn: convolution launch (%d row blocks, %d K-steps, %zu B shared) failed: %s", a.MT,
@@ -804,6 +827,24 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
 }
 
 static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, (long long)num_sms() * 16); }
+
+// 2x2 average pool between CG tensors, launched as a programmatic dependent of the convolution
+// before it
+static ufob_status pool_launch(const CGBuf &in, const CGBuf &out, int planes, long long n, cudaStream_t s)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid_for(n));
+    cfg.blockDim = dim3(256);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    UFOB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_cg_pool, (const bf16 *)in.ptr(), out.ptr(), in.g, out.g, planes));
+    note_launch();
+    return UFOB_OK;
+}
 
 void *cnn_fast_create() { return new FastNet; }
 void cnn_fast_destroy(void *p) { delete static_cast<FastNet *>(p); }
@@ -845,14 +886,11 @@ ufob_status cnn_fast_forward(void *fp, const float *const *bias, const float *fb
     note_launch();
     auto wt = [&](int i) { return f->wt[i].as<bf16>(); };
     UFOB_TRY(conv_cg(f, f->x0, wt(0), bias[0], 32, 1, EPI_STORE, &f->e1, nullptr, nullptr, nullptr, 0.f, s));
-    k_cg_pool<<<grid_for(npx / 4 * 4), 256, 0, s>>>(f->e1.ptr(), f->p1.ptr(), f->e1.g, f->p1.g, 4);
-    note_launch();
+    UFOB_TRY(pool_launch(f->e1, f->p1, 4, npx / 4 * 4, s));
     UFOB_TRY(conv_cg(f, f->p1, wt(1), bias[1], 64, 1, EPI_STORE, &f->e2, nullptr, nullptr, nullptr, 0.f, s));
-    k_cg_pool<<<grid_for(npx / 16 * 8), 256, 0, s>>>(f->e2.ptr(), f->p2.ptr(), f->e2.g, f->p2.g, 8);
-    note_launch();
+    UFOB_TRY(pool_launch(f->e2, f->p2, 8, npx / 16 * 8, s));
     UFOB_TRY(conv_cg(f, f->p2, wt(2), bias[2], 128, 1, EPI_STORE, &f->e3, nullptr, nullptr, nullptr, 0.f, s));
-    k_cg_pool<<<grid_for(npx / 64 * 16), 256, 0, s>>>(f->e3.ptr(), f->p3.ptr(), f->e3.g, f->p3.g, 16);
-    note_launch();
+    UFOB_TRY(pool_launch(f->e3, f->p3, 16, npx / 64 * 16, s));
     UFOB_TRY(conv_cg(f, f->p3, wt(3), bias[3], 256, 1, EPI_STORE, &f->e4, nullptr, nullptr, nullptr, 0.f, s));
     UFOB_TRY(conv_cg(f, f->e4, wt(4), bias[4], 128, 1, EPI_UPADD, &f->u3, &f->e3, nullptr, nullptr, 0.f, s));
     UFOB_TRY(conv_cg(f, f->u3, wt(5), bias[5], 64, 1, EPI_UPADD, &f->u2, &f->e2, nullptr, nullptr, 0.f, s));
