@@ -599,35 +599,39 @@ __global__ void __launch_bounds__(kThreads, 1) k_conv_cg(const FastConvArgs a)
 
 #define CG_LOOP(i, n) for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
+// The per-pixel kernels below run on a 2-D grid: y walks the images (slices, or channel planes x
+// slices), x one image's output pixels, so every index is 32-bit arithmetic (one image holds at
+// most 2^31 pixels; 64-bit divisions by runtime sizes cost more than these kernels' loads).
+
 // fbp [B][4H][4W] -> CG x0 (16 channels, two planes): channel 4*dy + dx = fbp[4y+dy][4x+dx] / s
 __global__ void k_cg_unshuffle(const float *__restrict__ fbp, bf16 *__restrict__ x0, CGGeom g, float inv_s)
 {
     pdl_launch_dependents();
-    const long long n = (long long)g.B * g.H * g.W;
-    CG_LOOP(i, n) {
-        const int x = (int)(i % g.W), y = (int)((i / g.W) % g.H);
-        const long long b = i / ((long long)g.W * g.H);
-        const size_t W4 = (size_t)4 * g.W;
-        const float *src = fbp + ((size_t)b * 4 * g.H + 4 * y) * W4 + 4 * x;
-        float v[16];
+    const uint32_t hw = (uint32_t)g.H * (uint32_t)g.W;
+    const size_t W4 = (size_t)4 * g.W;
+    for (uint32_t b = blockIdx.y; b < (uint32_t)g.B; b += gridDim.y)
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hw; i += gridDim.x * blockDim.x) {
+            const uint32_t y = i / (uint32_t)g.W, x = i - y * (uint32_t)g.W;
+            const float *src = fbp + ((size_t)b * 4 * g.H + 4 * y) * W4 + 4 * x;
+            float v[16];
 #pragma unroll
-        for (int dy = 0; dy < 4; dy++) {
-            const float4 f = *reinterpret_cast<const float4 *>(src + dy * W4);
-            v[4 * dy] = f.x * inv_s;
-            v[4 * dy + 1] = f.y * inv_s;
-            v[4 * dy + 2] = f.z * inv_s;
-            v[4 * dy + 3] = f.w * inv_s;
-        }
-        const long long q = (b * (g.H + 2) + y + 1) * (g.W + 2) + x + 1;
-        float lo[8], hi[8];
+            for (int dy = 0; dy < 4; dy++) {
+                const float4 f = *reinterpret_cast<const float4 *>(src + dy * W4);
+                v[4 * dy] = f.x * inv_s;
+                v[4 * dy + 1] = f.y * inv_s;
+                v[4 * dy + 2] = f.z * inv_s;
+                v[4 * dy + 3] = f.w * inv_s;
+            }
+            const long long q = ((long long)b * (g.H + 2) + y + 1) * (g.W + 2) + x + 1;
+            float lo[8], hi[8];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-            lo[k] = v[k];
-            hi[k] = v[8 + k];
+            for (int k = 0; k < 8; k++) {
+                lo[k] = v[k];
+                hi[k] = v[8 + k];
+            }
+            *reinterpret_cast<uint4 *>(x0 + ((size_t)g.guard + q) * 8) = pack8(lo);
+            *reinterpret_cast<uint4 *>(x0 + ((size_t)g.alloc + g.guard + q) * 8) = pack8(hi);
         }
-        *reinterpret_cast<uint4 *>(x0 + ((size_t)g.guard + q) * 8) = pack8(lo);
-        *reinterpret_cast<uint4 *>(x0 + ((size_t)g.alloc + g.guard + q) * 8) = pack8(hi);
-    }
 }
 
 // 2x2 average pool between CG tensors (gi -> go = gi / 2), C/8 planes
@@ -635,22 +639,29 @@ __global__ void k_cg_pool(const bf16 *__restrict__ in, bf16 *__restrict__ out, C
 {
     pdl_launch_dependents();
     pdl_wait();
-    const long long n = (long long)planes * go.B * go.H * go.W;
-    CG_LOOP(i, n) {
-        const int x = (int)(i % go.W), y = (int)((i / go.W) % go.H);
-        const long long r = i / ((long long)go.W * go.H);
-        const int b = (int)(r % go.B), p = (int)(r / go.B);
-        const long long qi = ((long long)b * (gi.H + 2) + 2 * y + 1) * (gi.W + 2) + 2 * x + 1;
-        const bf16 *s = in + ((size_t)p * gi.alloc + gi.guard + qi) * 8;
-        float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        unpack8_add(*reinterpret_cast<const uint4 *>(s), v);
-        unpack8_add(*reinterpret_cast<const uint4 *>(s + 8), v);
-        unpack8_add(*reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 2) * 8), v);
-        unpack8_add(*reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 3) * 8), v);
+    const uint32_t hw = (uint32_t)go.H * (uint32_t)go.W, images = (uint32_t)planes * (uint32_t)go.B;
+    for (uint32_t img = blockIdx.y; img < images; img += gridDim.y) {
+        const uint32_t p = img / (uint32_t)go.B, b = img - p * (uint32_t)go.B;
+        const bf16 *ip = in + ((size_t)p * gi.alloc + gi.guard) * 8;
+        bf16 *op = out + ((size_t)p * go.alloc + go.guard) * 8;
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < hw; i += gridDim.x * blockDim.x) {
+            const uint32_t y = i / (uint32_t)go.W, x = i - y * (uint32_t)go.W;
+            const long long qi = ((long long)b * (gi.H + 2) + 2 * y + 1) * (gi.W + 2) + 2 * x + 1;
+            const bf16 *s = ip + (size_t)qi * 8;
+            const uint4 r0 = *reinterpret_cast<const uint4 *>(s);
+            const uint4 r1 = *reinterpret_cast<const uint4 *>(s + 8);
+            const uint4 r2 = *reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 2) * 8);
+            const uint4 r3 = *reinterpret_cast<const uint4 *>(s + (size_t)(gi.W + 3) * 8);
+            float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            unpack8_add(r0, v);
+            unpack8_add(r1, v);
+            unpack8_add(r2, v);
+            unpack8_add(r3, v);
 #pragma unroll
-        for (int k = 0; k < 8; k++) v[k] *= 0.25f;
-        const long long qo = ((long long)b * (go.H + 2) + y + 1) * (go.W + 2) + x + 1;
-        *reinterpret_cast<uint4 *>(out + ((size_t)p * go.alloc + go.guard + qo) * 8) = pack8(v);
+            for (int k = 0; k < 8; k++) v[k] *= 0.25f;
+            const long long qo = ((long long)b * (go.H + 2) + y + 1) * (go.W + 2) + x + 1;
+            *reinterpret_cast<uint4 *>(op + (size_t)qo * 8) = pack8(v);
+        }
     }
 }
 
@@ -828,12 +839,19 @@ static ufob_status conv_cg(FastNet *f, const CGBuf &in, const bf16 *wt, const fl
 
 static unsigned grid_for(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, (long long)num_sms() * 16); }
 
+// 256-thread CTAs over one image's pixels (x) and the images (y)
+static dim3 grid_images(const CGGeom &g, int images)
+{
+    const unsigned hw = (unsigned)g.H * (unsigned)g.W;
+    return dim3((hw + 255) / 256, (unsigned)std::min(images, 65535));
+}
+
 // 2x2 average pool between CG tensors, launched as a programmatic dependent of the convolution
 // before it
-static ufob_status pool_launch(const CGBuf &in, const CGBuf &out, int planes, long long n, cudaStream_t s)
+static ufob_status pool_launch(const CGBuf &in, const CGBuf &out, int planes, cudaStream_t s)
 {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid_for(n));
+    cfg.gridDim = grid_images(out.g, planes * out.g.B);
     cfg.blockDim = dim3(256);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -880,17 +898,16 @@ ufob_status cnn_fast_forward(void *fp, const float *const *bias, const float *fb
     UFOB_TRY(cg_alloc(f->u3, B, H / 4, W / 4, 128, s));
     UFOB_TRY(cg_alloc(f->u2, B, H / 2, W / 2, 64, s));
     UFOB_TRY(cg_alloc(f->u1, B, H, W, 32, s));
-    const long long npx = (long long)B * H * W;
-    k_cg_unshuffle<<<grid_for(npx), 256, 0, s>>>(fbp, f->x0.ptr(), f->x0.g, 1.f / scale);
+    k_cg_unshuffle<<<grid_images(f->x0.g, B), 256, 0, s>>>(fbp, f->x0.ptr(), f->x0.g, 1.f / scale);
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     auto wt = [&](int i) { return f->wt[i].as<bf16>(); };
     UFOB_TRY(conv_cg(f, f->x0, wt(0), bias[0], 32, 1, EPI_STORE, &f->e1, nullptr, nullptr, nullptr, 0.f, s));
-    UFOB_TRY(pool_launch(f->e1, f->p1, 4, npx / 4 * 4, s));
+    UFOB_TRY(pool_launch(f->e1, f->p1, 4, s));
     UFOB_TRY(conv_cg(f, f->p1, wt(1), bias[1], 64, 1, EPI_STORE, &f->e2, nullptr, nullptr, nullptr, 0.f, s));
-    UFOB_TRY(pool_launch(f->e2, f->p2, 8, npx / 16 * 8, s));
+    UFOB_TRY(pool_launch(f->e2, f->p2, 8, s));
     UFOB_TRY(conv_cg(f, f->p2, wt(2), bias[2], 128, 1, EPI_STORE, &f->e3, nullptr, nullptr, nullptr, 0.f, s));
-    UFOB_TRY(pool_launch(f->e3, f->p3, 16, npx / 64 * 16, s));
+    UFOB_TRY(pool_launch(f->e3, f->p3, 16, s));
     UFOB_TRY(conv_cg(f, f->p3, wt(3), bias[3], 256, 1, EPI_STORE, &f->e4, nullptr, nullptr, nullptr, 0.f, s));
     UFOB_TRY(conv_cg(f, f->e4, wt(4), bias[4], 128, 1, EPI_UPADD, &f->u3, &f->e3, nullptr, nullptr, 0.f, s));
     UFOB_TRY(conv_cg(f, f->u3, wt(5), bias[5], 64, 1, EPI_UPADD, &f->u2, &f->e2, nullptr, nullptr, 0.f, s));
