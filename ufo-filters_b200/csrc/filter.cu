@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "tma.cuh"
 #include "ufob_internal.h"
 
 namespace ufob {
@@ -620,32 +621,70 @@ __device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 
     return a;
 }
 
-template <int OUT, bool PRE, int LOGN>
+// With STG, each team's two input rows of the next work item are fetched by bulk copies into a
+// staging buffer while the current item is transformed (one mbarrier per team, bounded waits),
+// so the first pass reads shared memory instead of waiting on global loads; the host selects it
+// for plain FP32 rows whose starts and lengths are 16-byte multiples when it costs no resident CTA.
+template <int OUT, bool PRE, int LOGN, bool STG>
 __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource src, uint32_t width, uint32_t rows,
                                                              const float2 *__restrict__ g_tab,
                                                              const float2 *__restrict__ g_gains,
                                                              void *__restrict__ out, uint32_t out_w,
-                                                             uint32_t out_pitch, uint32_t npairs, uint32_t P)
+                                                             uint32_t out_pitch, uint32_t npairs, uint32_t P,
+                                                             int *__restrict__ err)
 {
     constexpr uint32_t N = 1u << LOGN, T = N / 16, TEAMS = kFastThreads / T;
     constexpr uint32_t R3 = N / 256, LR3 = R3 >= 16 ? 4 : R3 >= 8 ? 3 : R3 >= 4 ? 2 : R3 >= 2 ? 1 : 0;
     constexpr uint32_t NTAB = 4 * 16 + LR3 * 256;
+    static_assert(!(STG && PRE), "staged rows carry no preprocessing");
     extern __shared__ float4 smem_f4[];
+    __shared__ uint64_t s_bar[TEAMS];
     float2 *sm = reinterpret_cast<float2 *>(smem_f4);
     float2 *tab2 = sm, *tab3 = sm + 64, *gains = sm + NTAB;
     const uint32_t team = threadIdx.x / T, t = threadIdx.x - team * T;
     float2 *bufA = gains + (N / 2 + 2) + team * 2 * N, *bufB = bufA + N;
+    float *stg = reinterpret_cast<float *>(gains + (N / 2 + 2) + TEAMS * 2 * N) + team * 2 * N;
     for (uint32_t i = threadIdx.x; i < NTAB; i += kFastThreads) sm[i] = g_tab[i];
     for (uint32_t i = threadIdx.x; i <= N / 2; i += kFastThreads) gains[i] = g_gains[i];
 
     const uint32_t iters = (npairs + gridDim.x * TEAMS - 1) / (gridDim.x * TEAMS);
+    const uint32_t wl = width < N ? width : N;  // samples read per row
+    // leader of the team: expect and issue the rows of iteration i (nothing for a pair past the
+    // end; a row past the stack is not copied and reads as zero)
+    auto issue = [&](uint32_t i) {
+        const uint32_t pr = (i * gridDim.x + blockIdx.x) * TEAMS + team;
+        if (pr >= npairs) return;
+        const PairMap mm = map_pair<OUT>(pr, rows, P, out_pitch);
+        uint32_t y, p;
+        mbar_arrive_expect_tx(&s_bar[team], ((mm.hasa ? 1u : 0u) + (mm.hasb ? 1u : 0u)) * wl * 4u);
+        if (mm.hasa) bulk_load_1d(stg, row_start(src, mm.ra, y, p), wl * 4u, &s_bar[team]);
+        if (mm.hasb) bulk_load_1d(stg + N, row_start(src, mm.rb, y, p), wl * 4u, &s_bar[team]);
+    };
+    if (STG) {
+        if (t == 0) {
+            mbar_init(&s_bar[team], 1);
+            fence_barrier_init();
+        }
+        __syncthreads();
+        if (t == 0 && iters > 0) issue(0);
+    }
     for (uint32_t it = 0; it < iters; it++) {
         const uint32_t pair = (it * gridDim.x + blockIdx.x) * TEAMS + team;
         const bool live = pair < npairs;
         const PairMap m = map_pair<OUT>(live ? pair : 0, live ? rows : 0, P, out_pitch);
-        // pass 1 loads straight from global memory: elements t + m N/16 of rows a, b
+        // pass 1 loads elements t + m N/16 of rows a, b (staged, or straight from global memory)
         float2 v[16];
-        {
+        bool failed = false;
+        if (STG) {
+            // live pairs come first in every team, so the barrier's phase is the iteration's parity
+            if (live && !mbar_wait_bounded(&s_bar[team], it & 1u, kWaitLimitNs)) failed = true;
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const uint32_t n = t + q * T;
+                const bool in = n < wl;
+                v[q] = make_float2(in && m.hasa ? stg[n] : 0.f, in && m.hasb ? stg[N + n] : 0.f);
+            }
+        } else {
             uint32_t ya, pa_, yb, pb_;
             const float *ra = row_start(src, m.hasa ? m.ra : 0, ya, pa_);
             const float *rb = row_start(src, m.hasb ? m.rb : 0, yb, pb_);
@@ -701,7 +740,17 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
                 }
             }
         }
-        __syncthreads();  // tables loaded; the previous item's output reads are done
+        // tables loaded; the previous item's output reads and this item's staged reads are done
+        if (STG) {
+            if (__syncthreads_or(failed)) {
+                if (threadIdx.x == 0) atomicExch(err, kErrTmaTimeout);
+                if (t == 0) mbar_wait_bounded(&s_bar[team], it & 1u, kWaitLimitNs);  // the copy in flight
+                return;
+            }
+            if (t == 0 && it + 1 < iters) issue(it + 1);
+        } else {
+            __syncthreads();
+        }
         dft<16, false>(v);
 #pragma unroll
         for (int q = 0; q < 16; q++) bufA[swz(t * 16 + q)] = v[q];
@@ -787,24 +836,59 @@ static ufob_status launch_rows_t(const FilterPlan &plan, const RowSource &src, u
     return UFOB_OK;
 }
 
+// Shared memory of k_filter_fast: pass twiddles, gains, two exchange buffers per team and, when
+// rows are staged, two input rows per team.
+template <int LOGN, bool STG>
+static size_t fast_smem()
+{
+    constexpr uint32_t N = 1u << LOGN, TEAMS = kFastThreads / (N / 16);
+    return sizeof(float2) * (pass_twiddle_count(N) + N / 2 + 2 + (size_t)TEAMS * 2 * N) +
+           (STG ? sizeof(float) * TEAMS * 2 * N : 0);
+}
+
+template <int OUT, bool PRE, int LOGN, bool STG>
+static ufob_status fast_occupancy(int &per_sm)
+{
+    auto kern = k_filter_fast<OUT, PRE, LOGN, STG>;
+    static std::atomic<uint64_t> attr_devs{0};
+    UFOB_CUDA_TRY(smem_limit_per_device(kern, (int)fast_smem<LOGN, STG>(), attr_devs));
+    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, fast_smem<LOGN, STG>()));
+    return UFOB_OK;
+}
+
+// Bulk copies need 16-byte aligned row starts and lengths.
+static bool rows_stageable(const RowSource &src, uint32_t width, uint32_t N)
+{
+    const uint32_t wl = std::min(width, N);
+    return !src.has_pre() && wl % 4 == 0 && ((uintptr_t)src.base & 15u) == 0 && src.outer_stride % 4 == 0 &&
+           src.inner_stride % 4 == 0;
+}
+
 template <int OUT, bool PRE, int LOGN>
 static ufob_status launch_fast_t(const FilterPlan &plan, const RowSource &src, uint32_t width, uint32_t rows,
                                  void *d_out, uint32_t out_w, uint32_t out_pitch, cudaStream_t s, uint32_t P)
 {
     constexpr uint32_t N = 1u << LOGN, TEAMS = kFastThreads / (N / 16);
-    const size_t smem = sizeof(float2) * (pass_twiddle_count(N) + N / 2 + 2 + (size_t)TEAMS * 2 * N);
-    auto kern = k_filter_fast<OUT, PRE, LOGN>;
-    static std::atomic<uint64_t> attr_devs{0};
-    UFOB_CUDA_TRY(smem_limit_per_device(kern, (int)smem, attr_devs));
-    int per_sm = 0;
-    UFOB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kFastThreads, smem));
+    int per_sm = 0, per_sm_stg = 0;
+    UFOB_TRY((fast_occupancy<OUT, PRE, LOGN, false>(per_sm)));
     if (per_sm < 1) return fail(UFOB_ERR_UNSUPPORTED, "filter: FFT width %u does not fit in shared memory", N);
+    // stage the rows only where the staging buffers cost no resident CTA
+    bool stg = !PRE && rows_stageable(src, width, N);
+    if (stg) {
+        UFOB_TRY((fast_occupancy<OUT, false, LOGN, true>(per_sm_stg)));
+        stg = per_sm_stg >= per_sm;
+    }
     const uint32_t npairs = OUT == OUT_F16_QUADS ? (rows / P + 3) / 4 * P * 2 : (rows + 1) / 2;
     uint32_t grid = (uint32_t)num_sms() * (uint32_t)per_sm;
     grid = std::min(grid, (npairs + TEAMS - 1) / TEAMS);
     if (grid == 0) return UFOB_OK;
-    kern<<<grid, kFastThreads, smem, s>>>(src, width, rows, plan.d_pass_tw.as<float2>(), plan.d_gains.as<float2>(),
-                                          d_out, out_w, out_pitch, npairs, P);
+    const float2 *tab = plan.d_pass_tw.as<float2>(), *gains = plan.d_gains.as<float2>();
+    if (stg)
+        k_filter_fast<OUT, false, LOGN, true><<<grid, kFastThreads, fast_smem<LOGN, true>(), s>>>(
+            src, width, rows, tab, gains, d_out, out_w, out_pitch, npairs, P, device_error_word());
+    else
+        k_filter_fast<OUT, PRE, LOGN, false><<<grid, kFastThreads, fast_smem<LOGN, false>(), s>>>(
+            src, width, rows, tab, gains, d_out, out_w, out_pitch, npairs, P, device_error_word());
     UFOB_CUDA_TRY(cudaGetLastError());
     note_launch();
     return UFOB_OK;
