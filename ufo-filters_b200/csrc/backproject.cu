@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "f32x2.cuh"
 #include "tma.cuh"
 #include "ufob_internal.h"
 
@@ -188,38 +189,6 @@ __device__ __forceinline__ void fma2(float &a0, float &a1, float k, float x0, fl
         "fma.rn.f32x2 a, kk, x, a;\n\tmov.b64 {%0, %1}, a;\n\t}"
         : "+f"(a0), "+f"(a1)
         : "f"(x0), "f"(x1), "f"(k));
-}
-
-// Packed FP32 pairs (sm_100 f32x2 arithmetic; each lane rounds exactly as the
-// scalar instruction does, so the packed chains below are bit-identical to
-// their scalar forms).
-__device__ __forceinline__ uint64_t f2pack(float lo, float hi)
-{
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-__device__ __forceinline__ void f2unpack(uint64_t v, float &lo, float &hi)
-{
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c)
-{
-    uint64_t r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-__device__ __forceinline__ uint64_t f2add(uint64_t a, uint64_t b)
-{
-    uint64_t r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b)
-{
-    uint64_t r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
 }
 
 // acc += w_lo * s_lo + w_hi * s_hi with 16-bit operands and FP32 accumulation

@@ -35,6 +35,7 @@
 #include <cmath>
 #include <string>
 
+#include "f32x2.cuh"
 #include "tma.cuh"
 #include "ufob_internal.h"
 
@@ -488,9 +489,11 @@ __global__ void __launch_bounds__(256) k_gbp(const GBPArgs a)
 // in z per projection.  A CTA owns 32 x 8 columns of ZT voxels.  Per projection
 // the detector window its samples reach (bw x bh texels, bw a multiple of 4,
 // from the host's plan) is staged by one TMA copy into an S-stage ring of PB
-// projections per stage (warp 0 finds the windows, one lane per projection;
-// each warp releases a stage through an mbarrier, so warps drift up to S - 1
-// stages apart instead of meeting at a CTA barrier per stage).  Samples are
+// projections per stage (warp 0 finds the windows, one lane per projection,
+// from the stage's tables, which a bulk copy brought into a ring of S + 1 table
+// slots one stage earlier; each warp releases a stage through an mbarrier, so
+// warps drift up to S - 1 stages apart instead of meeting at a CTA barrier per
+// stage).  Samples are
 // interpolated from shared memory with exact FP32 weights (floor and fraction
 // by the round-down 1.5 * 2^23 trick, v' = v - 1/2 one affine function of z per
 // column).  TMA's zero fill outside the detector is the reference's CLAMP
@@ -511,22 +514,25 @@ struct GBPColArgs {
 template <int PB, int S>
 struct GBPColSmem {
     float *data;     // [S][PB][slot_floats] staged windows
-    float4 *tab;     // [S][PB][kTab / 4] tables of the staged projections
+    float4 *tab;     // [S + 1][PB][kTab / 4] tables of the staged projections (one stage ahead)
     int2 *org;       // [S][PB] window origin (u0, v0) in texels
-    uint64_t *full;  // [S] mbarriers: the stage's copies have landed
+    uint64_t *full;  // [S] mbarriers: the stage's window copies have landed
     uint64_t *empty; // [S] mbarriers: all 8 warps are done with the stage
+    uint64_t *tfull; // [S + 1] mbarriers: the table slot's copy has landed
     static size_t bytes(uint32_t slot_floats)
     {
-        return (size_t)S * PB * slot_floats * 4 + (size_t)S * PB * kTab * 4 + (size_t)S * PB * 8 + (size_t)S * 16 + 128;
+        return (size_t)S * PB * slot_floats * 4 + (size_t)(S + 1) * PB * kTab * 4 + (size_t)S * PB * 8 +
+               (size_t)(3 * S + 1) * 8 + 128;
     }
     __device__ __forceinline__ GBPColSmem(unsigned char *dyn, uint32_t slot_floats)
     {
         unsigned char *raw = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(dyn) + 127) & ~(uintptr_t)127);
         data = reinterpret_cast<float *>(raw);
         tab = reinterpret_cast<float4 *>(data + (size_t)S * PB * slot_floats);
-        org = reinterpret_cast<int2 *>(tab + S * PB * (kTab / 4));
+        org = reinterpret_cast<int2 *>(tab + (S + 1) * PB * (kTab / 4));
         full = reinterpret_cast<uint64_t *>(org + S * PB);
         empty = full + S;
+        tfull = empty + S;
     }
 };
 
@@ -534,6 +540,7 @@ template <bool CONE, int ZT, int PB, int S>
 __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUtensorMap map, const GBPColArgs c)
 {
     static_assert(PB <= 32 && kTab % 4 == 0, "one producer lane per projection of a stage");
+    static_assert(ZT % 2 == 0, "the voxels of a column are processed in packed pairs");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     const GBPColSmem<PB, S> sm(smem_dyn, c.slot_floats);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -541,34 +548,48 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
     // a warp covers 16 x 2 columns: its samples of one row then span fewer than 32 banks
     const int ix = x0 + (warp & 1) * 16 + (lane & 15), iy = y0 + (warp >> 1) * 2 + (lane >> 4);
     const float fx = (float)ix, fy = (float)iy;
-    float zv[ZT];
+    // z of the column's voxels as packed pairs (2j, 2j + 1)
+    uint64_t zz[ZT / 2];
 #pragma unroll
-    for (int k = 0; k < ZT; k++) zv[k] = (float)c.zvals[min(z0 + k, (int)c.nz - 1)];
-    const float zlo = zv[0], zhi = zv[ZT - 1];
+    for (int j = 0; j < ZT / 2; j++)
+        zz[j] = f2pack((float)c.zvals[min(z0 + 2 * j, (int)c.nz - 1)], (float)c.zvals[min(z0 + 2 * j + 1, (int)c.nz - 1)]);
+    float zlo, zhi, zdummy;
+    f2unpack(zz[0], zlo, zdummy);
+    f2unpack(zz[ZT / 2 - 1], zdummy, zhi);
     if (tid == 0) {
         for (int q = 0; q < S; q++) {
             mbar_init(&sm.full[q], 1);
             mbar_init(&sm.empty[q], 8);
         }
+        for (int q = 0; q <= S; q++) mbar_init(&sm.tfull[q], 1);
         fence_barrier_init();
     }
     __syncthreads();
 
     const int n = (int)c.n_proj, nblk = (n + PB - 1) / PB;
+    // lane 0 of warp 0: bulk copy of the tables of stage blk (contiguous, 80 bytes each) into
+    // table slot blk % (S + 1), whose previous stage (blk - S - 1) every warp has released
+    auto issue_tab = [&](int blk) {
+        const int ts = blk % (S + 1), nval = min(PB, n - blk * PB);
+        mbar_arrive_expect_tx(&sm.tfull[ts], (uint32_t)nval * kTab * 4u);
+        bulk_load_1d(sm.tab + ts * PB * (kTab / 4), c.tab + (size_t)blk * PB * kTab, (uint32_t)nval * kTab * 4u,
+                     &sm.tfull[ts]);
+    };
     // Producer, all lanes of warp 0: lane q stages projection blk * PB + q once every warp has
-    // released the slot's previous stage.  Returns false if that wait gave up.
+    // released the slot's previous stage, and the tables of stage blk + 1 are requested.
+    // Returns false if a wait gave up.
     auto issue = [&](int blk) {
-        const int slot = blk % S, p = blk * PB + lane;
+        const int slot = blk % S, ts = blk % (S + 1), p = blk * PB + lane;
         const int nval = min(PB, n - blk * PB);
         if (blk >= S && !mbar_wait_bounded(&sm.empty[slot], (uint32_t)(blk / S - 1) & 1u, kWaitLimitNs)) return false;
+        if (lane == 0 && blk + 1 < nblk) issue_tab(blk + 1);
+        if (!mbar_wait_bounded(&sm.tfull[ts], (uint32_t)(blk / (S + 1)) & 1u, kWaitLimitNs)) return false;
         int u0 = 0, v0 = 0;
         if (lane < nval) {
-            const float4 *tr = reinterpret_cast<const float4 *>(c.tab + (size_t)p * kTab);
             float t[kTab];
 #pragma unroll
             for (int r = 0; r < kTab / 4; r++) {
-                const float4 w = __ldg(tr + r);
-                sm.tab[(slot * PB + lane) * (kTab / 4) + r] = w;
+                const float4 w = sm.tab[(ts * PB + lane) * (kTab / 4) + r];
                 t[4 * r] = w.x;
                 t[4 * r + 1] = w.y;
                 t[4 * r + 2] = w.z;
@@ -611,8 +632,11 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
         if (lane < nval) tma_load_3d(sm.data + (size_t)(slot * PB + lane) * c.slot_floats, &map, &sm.full[slot], u0, v0, p);
         return true;
     };
+    if (tid == 0 && nblk > 0) issue_tab(0);
+    bool aborted = false;
     if (tid < 32)
-        for (int b = 0; b < S - 1 && b < nblk; b++) issue(b);
+        for (int b = 0; b < S - 1 && b < nblk; b++)
+            if (!issue(b)) aborted = true;
 
     const float M1 = 12582911.0f;  // 1.5 * 2^23 - 1: (x + M1) - M1 = rint(x) for |x| < 2^22
     const int M1b = __float_as_int(M1);
@@ -620,19 +644,23 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
     const int Mb = __float_as_int(M);
     const float Wf = (float)c.W + 2.0f, Hf = (float)c.H + 2.0f;
     const int bw = (int)c.bw;
-    float acc[ZT], bsum[ZT];
+    float acc[ZT];
+    uint64_t bsum[ZT / 2];  // burst sums of voxels (2j, 2j + 1)
 #pragma unroll
-    for (int k = 0; k < ZT; k++) acc[k] = bsum[k] = 0.f;
+    for (int k = 0; k < ZT; k++) acc[k] = 0.f;
+#pragma unroll
+    for (int j = 0; j < ZT / 2; j++) bsum[j] = 0;  // (+0, +0)
     uint32_t in_burst = 0;
-    bool aborted = false;
-    for (int blk = 0; blk < nblk; blk++) {
+    for (int blk = 0; blk < nblk && !aborted; blk++) {
         // the warps run up to S - 1 stages apart: no CTA-wide barrier per stage
         if (tid < 32 && blk + S - 1 < nblk && !issue(blk + S - 1)) {
             aborted = true;
             break;
         }
-        const int slot = blk % S;
-        const bool ok = mbar_wait_bounded(&sm.full[slot], (uint32_t)(blk / S) & 1u, kWaitLimitNs);
+        const int slot = blk % S, ts = blk % (S + 1);
+        // the stage's windows, and its tables (whose copy the producer saw land before it issued them)
+        const bool ok = mbar_wait_bounded(&sm.full[slot], (uint32_t)(blk / S) & 1u, kWaitLimitNs) &&
+                        mbar_wait_bounded(&sm.tfull[ts], (uint32_t)(blk / (S + 1)) & 1u, kWaitLimitNs);
         const int nval = min(PB, n - blk * PB);
         if (ok) {
             for (int q = 0; q < nval; q++) {
@@ -640,7 +668,7 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
                 float t[kTab];
 #pragma unroll
                 for (int r = 0; r < kTab / 4; r++)
-                    *reinterpret_cast<float4 *>(&t[4 * r]) = sm.tab[(slot * PB + q) * (kTab / 4) + r];
+                    *reinterpret_cast<float4 *>(&t[4 * r]) = sm.tab[(ts * PB + q) * (kTab / 4) + r];
                 const int2 o = sm.org[slot * PB + q];
                 const float *win = sm.data + (size_t)(slot * PB + q) * c.slot_floats;
                 const float uxy = fmaf(t[0], fx, fmaf(t[1], fy, t[3]));
@@ -656,7 +684,8 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
                 if (o.x != INT_MIN) {
                     // the tile's footprints lie inside the staged window (one guard texel each side):
                     // x' = x - 0.5 per axis, tap = floor(x') by adding 1.5 * 2^23 rounded down,
-                    // weight = x' - tap; v' is affine in z: v' = Av * z + Bv
+                    // weight = x' - tap; v' is affine in z: v' = Av * z + Bv.  Two voxels of the
+                    // column per packed FP32 operation (each lane rounds as the scalar form).
                     const float up = fmaf(uxy, inv, -0.5f);
                     const float ru = __fadd_rd(up, M);
                     const float a = up - (ru - M);
@@ -664,17 +693,25 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
                     const float Av = t[6] * inv, Bv = fmaf(vxy, inv, -0.5f);
                     const int vbase = Mb + o.y;
                     const float *col = win + iu;
+                    const uint64_t AA = f2pack(a, a), AV = f2pack(Av, Av), BV = f2pack(Bv, Bv);
+                    const uint64_t MM = f2pack(M, M), WG = f2pack(wgt, wgt);
 #pragma unroll
-                    for (int k = 0; k < ZT; k++) {
-                        const float vp = fmaf(Av, zv[k], Bv);
-                        const float rv = __fadd_rd(vp, M);
-                        const float b = vp - (rv - M);
-                        const int iv = min(max(__float_as_int(rv) - vbase, 0), (int)c.bh - 2);
-                        const float *sp = col + iv * bw;
-                        const float t00 = sp[0], t10 = sp[1], t01 = sp[bw], t11 = sp[bw + 1];
-                        const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
-                        const float val = fmaf(b, bot - top, top);
-                        bsum[k] = CONE ? fmaf(val, wgt, bsum[k]) : bsum[k] + val;
+                    for (int j = 0; j < ZT / 2; j++) {
+                        const uint64_t vp = f2fma(AV, zz[j], BV);
+                        const uint64_t rv = f2add_rd(vp, MM);
+                        const uint64_t bb = f2sub(vp, f2sub(rv, MM));
+                        float r0, r1;
+                        f2unpack(rv, r0, r1);
+                        // one unsigned clamp keeps every read inside the window (the plan's guard
+                        // texels already do for every in-range footprint)
+                        const uint32_t i0 = min((uint32_t)(__float_as_int(r0) - vbase), c.bh - 2u);
+                        const uint32_t i1 = min((uint32_t)(__float_as_int(r1) - vbase), c.bh - 2u);
+                        const float *p0 = col + i0 * (uint32_t)bw, *p1 = col + i1 * (uint32_t)bw;
+                        const uint64_t t00 = f2pack(p0[0], p1[0]), t10 = f2pack(p0[1], p1[1]);
+                        const uint64_t t01 = f2pack(p0[bw], p1[bw]), t11 = f2pack(p0[bw + 1], p1[bw + 1]);
+                        const uint64_t top = f2fma(AA, f2sub(t10, t00), t00), bot = f2fma(AA, f2sub(t11, t01), t01);
+                        const uint64_t val = f2fma(bb, f2sub(bot, top), top);
+                        bsum[j] = CONE ? f2fma(val, WG, bsum[j]) : f2add(bsum[j], val);
                     }
                 } else {
                     // window not staged: the same footprints and weights from global memory
@@ -686,23 +723,32 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
                     auto texel0 = [&](int i, int j) {
                         return ((unsigned)i < c.W && (unsigned)j < c.H) ? __ldg(img + (size_t)j * c.W + i) : 0.f;
                     };
-                    for (int k = 0; k < ZT; k++) {
-                        const float v = fminf(fmaxf(fmaf(t[6], zv[k], vxy) * inv, -2.0f), Hf);
-                        const float rv = v + M1;
-                        const float b = (v + 0.5f) - (rv - M1);
-                        const int j0 = __float_as_int(rv) - M1b - 1;
-                        const float t00 = texel0(i0, j0), t10 = texel0(i0 + 1, j0);
-                        const float t01 = texel0(i0, j0 + 1), t11 = texel0(i0 + 1, j0 + 1);
-                        const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
-                        const float val = fmaf(b, bot - top, top);
-                        bsum[k] = CONE ? fmaf(val, wgt, bsum[k]) : bsum[k] + val;
+                    for (int j = 0; j < ZT / 2; j++) {
+                        float zp[2], bs[2];
+                        f2unpack(zz[j], zp[0], zp[1]);
+                        f2unpack(bsum[j], bs[0], bs[1]);
+                        for (int h = 0; h < 2; h++) {
+                            const float v = fminf(fmaxf(fmaf(t[6], zp[h], vxy) * inv, -2.0f), Hf);
+                            const float rv = v + M1;
+                            const float b = (v + 0.5f) - (rv - M1);
+                            const int j0 = __float_as_int(rv) - M1b - 1;
+                            const float t00 = texel0(i0, j0), t10 = texel0(i0 + 1, j0);
+                            const float t01 = texel0(i0, j0 + 1), t11 = texel0(i0 + 1, j0 + 1);
+                            const float top = fmaf(a, t10 - t00, t00), bot = fmaf(a, t11 - t01, t01);
+                            const float val = fmaf(b, bot - top, top);
+                            bs[h] = CONE ? fmaf(val, wgt, bs[h]) : bs[h] + val;
+                        }
+                        bsum[j] = f2pack(bs[0], bs[1]);
                     }
                 }
                 if (++in_burst == c.burst || p + 1 == n) {
 #pragma unroll
-                    for (int k = 0; k < ZT; k++) {
-                        acc[k] = acc[k] + __fmul_rn(c.norm, bsum[k]);
-                        bsum[k] = 0.f;
+                    for (int j = 0; j < ZT / 2; j++) {
+                        float b0, b1;
+                        f2unpack(bsum[j], b0, b1);
+                        acc[2 * j] = acc[2 * j] + __fmul_rn(c.norm, b0);
+                        acc[2 * j + 1] = acc[2 * j + 1] + __fmul_rn(c.norm, b1);
+                        bsum[j] = 0;
                     }
                     in_burst = 0;
                 }
@@ -722,6 +768,8 @@ __global__ void __launch_bounds__(256, 2) k_gbp_col(const __grid_constant__ CUte
             atomicExch(c.err, kErrTmaTimeout);
             for (int q = 0; q < S; q++)
                 for (int k = 0; k < 2; k++) mbar_wait_bounded(&sm.full[q], (uint32_t)k, kWaitLimitNs / 8);
+            for (int q = 0; q <= S; q++)
+                for (int k = 0; k < 2; k++) mbar_wait_bounded(&sm.tfull[q], (uint32_t)k, kWaitLimitNs / 8);
         }
         return;
     }
