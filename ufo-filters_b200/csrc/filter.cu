@@ -587,7 +587,11 @@ __device__ __forceinline__ void twiddle(float2 *v, const float2 *tab, uint32_t k
 
 // One Stockham pass (Ns > 1) of radix R over N points, shared src -> shared dst;
 // thread t of a team of T handles butterflies t, t + T, ... (16 / R of them).
-template <int R, bool INV>
+// LIN writes dst in natural order: the last pass of a transform stores runs of
+// consecutive elements across lanes, conflict-free without the swizzle, and a
+// linear result serves the filter step's mirrored reads and the output's
+// (j - 1, j) reads without bank conflicts.
+template <int R, bool INV, bool LIN>
 __device__ __forceinline__ void fast_pass(const float2 *src, float2 *dst, const float2 *tab, uint32_t N, uint32_t Ns,
                                           uint32_t t, uint32_t T)
 {
@@ -602,21 +606,22 @@ __device__ __forceinline__ void fast_pass(const float2 *src, float2 *dst, const 
         dft<R, INV>(v);
         const uint32_t base = (j - k) * R + k;
 #pragma unroll
-        for (int m = 0; m < R; m++) dst[swz(base + m * Ns)] = v[m];
+        for (int m = 0; m < R; m++) dst[LIN ? base + m * Ns : swz(base + m * Ns)] = v[m];
     }
 }
 
-// Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer.
+// Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer,
+// which holds the transform in natural (unswizzled) order.
 template <int LOGN, bool INV>
 __device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 *tab2, const float2 *tab3,
                                              uint32_t t, uint32_t T)
 {
     constexpr uint32_t N = 1u << LOGN;
     constexpr int R3 = (int)(N / 256);
-    fast_pass<16, INV>(a, b, tab2, N, 16, t, T);
+    fast_pass<16, INV, R3 == 1>(a, b, tab2, N, 16, t, T);
     __syncthreads();
     if (R3 == 1) return b;
-    fast_pass<(R3 > 1 ? R3 : 2), INV>(b, a, tab3, N, 256, t, T);
+    fast_pass<(R3 > 1 ? R3 : 2), INV, true>(b, a, tab3, N, 256, t, T);
     __syncthreads();
     return a;
 }
@@ -762,7 +767,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         for (int q = 0; q < 16; q++) {
             const uint32_t e = t + q * T;
             const uint32_t k = e <= N / 2 ? e : N - e;
-            const float2 zk = Z[swz(k)], zm = Z[swz((N - k) & (N - 1))], g = gains[k];
+            const float2 zk = Z[k], zm = Z[(N - k) & (N - 1)], g = gains[k];
             float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
             float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
             ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
@@ -773,7 +778,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
         __syncthreads();
         const float2 *X = fast_tail<LOGN, true>(O, O == bufA ? bufB : bufA, tab2, tab3, t, T);
-        if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[swz(i)]; }, out, out_w, out_pitch, t, T);
+        if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, t, T);
     }
 }
 
