@@ -778,7 +778,33 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
         __syncthreads();
         const float2 *X = fast_tail<LOGN, true>(O, O == bufA ? bufB : bufA, tab2, tab3, t, T);
-        if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, t, T);
+        if constexpr (OUT == OUT_F16_QUADS && TEAMS % 2 == 0) {
+            // teams 2u and 2u + 1 hold the two halves (slices 4g, 4g+1 and 4g+2, 4g+3 at one angle)
+            // of the same cells, and the barrier that ended the transform made both results visible:
+            // the pair's 2T threads write whole 16-byte cells, consecutive across threads
+            if (live) {
+                const uint32_t u = team >> 1, i0 = threadIdx.x - u * 2 * T;
+                const uint32_t pair0 = pair - (team & 1u);
+                const PairMap m0 = map_pair<OUT>(pair0, rows, P, out_pitch);
+                const PairMap m1 = map_pair<OUT>(pair0 + 1, rows, P, out_pitch);
+                const size_t xoff = (size_t)(X - bufA);  // this team's result: bufA or bufB
+                const float2 *X0 = gains + (N / 2 + 2) + (size_t)(2 * u) * 2 * N + xoff;
+                const float2 *X1 = X0 + 2 * N;
+                uint4 *o = reinterpret_cast<uint4 *>(out) + m0.cell0;
+                auto taps = [&](const float2 *Xh, const PairMap &mh, uint32_t j, bool prev) {
+                    const uint32_t e = prev ? j - 1 : j;
+                    float2 v = ((!prev || j >= 1) && e < out_w) ? Xh[e] : make_float2(0.f, 0.f);
+                    if (!mh.hasa) v.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
+                    if (!mh.hasb) v.y = 0.f;
+                    return pack_pair<OUT>(v.x, v.y);
+                };
+                for (uint32_t j = i0; j < out_pitch; j += 2 * T)
+                    o[j] = make_uint4(taps(X0, m0, j, true), taps(X1, m1, j, true), taps(X0, m0, j, false),
+                                      taps(X1, m1, j, false));
+            }
+        } else {
+            if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, t, T);
+        }
     }
 }
 
