@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cstdlib>
 
+#include "f32x2.cuh"
 #include "tma.cuh"
 #include "ufob_internal.h"
 
@@ -241,8 +242,19 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex add / subtract as one packed FP32 operation (each lane rounds as the scalar add)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b)
+{
+    float2 r;
+    f2unpack(f2add(f2pack(a.x, a.y), f2pack(b.x, b.y)), r.x, r.y);
+    return r;
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b)
+{
+    float2 r;
+    f2unpack(f2sub(f2pack(a.x, a.y), f2pack(b.x, b.y)), r.x, r.y);
+    return r;
+}
 
 // One Stockham pass of radix R over N points: src -> dst (both shared).
 // Twiddle for leg r of butterfly j in a sub-transform of size Ns*R is
@@ -494,11 +506,18 @@ __device__ __forceinline__ float2 mulc(float2 a, float c, float s)
 template <bool INV>
 __device__ __forceinline__ void dft4(float2 &x0, float2 &x1, float2 &x2, float2 &x3)
 {
-    const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<INV>(csub(x1, x3));
+    const float2 t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), d = csub(x1, x3);
     x0 = cadd(t0, t2);
     x2 = csub(t0, t2);
-    x1 = cadd(t1, t3);
-    x3 = csub(t1, t3);
+    // t3 = d * (-i) forward, d * (+i) inverse; x1 = t1 + t3 and x3 = t1 - t3 cross the lanes, so they
+    // stay scalar (a + (-b) and a - b round alike)
+    if (!INV) {
+        x1 = make_float2(t1.x + d.y, t1.y - d.x);
+        x3 = make_float2(t1.x - d.y, t1.y + d.x);
+    } else {
+        x1 = make_float2(t1.x - d.y, t1.y + d.x);
+        x3 = make_float2(t1.x + d.y, t1.y - d.x);
+    }
 }
 
 // In-place DFT of R points in natural order (R = 2, 4, 8, 16), forward e^{-2 pi i nk/R}.
