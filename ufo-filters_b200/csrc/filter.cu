@@ -785,12 +785,18 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
 #pragma unroll
         for (int q = 0; q < 16; q++) {
             const uint32_t e = t + q * T;
-            const uint32_t k = e <= N / 2 ? e : N - e;
+            const bool lower = e <= N / 2;
+            const uint32_t k = lower ? e : N - e;
             const float2 zk = Z[k], zm = Z[(N - k) & (N - 1)], g = gains[k];
-            float ax = 0.5f * (zk.x + zm.x), ay = 0.5f * (zk.y - zm.y);
-            float bx = 0.5f * (zk.y + zm.y), by = -0.5f * (zk.x - zm.x);
-            ax *= g.x; ay *= g.y; bx *= g.x; by *= g.y;
-            v[q] = e <= N / 2 ? make_float2(ax - by, ay + bx) : make_float2(ax + by, bx - ay);
+            // a = (zk + conj zm) / 2, b = (zk - conj zm) / 2i are the two rows' spectra at k; with
+            // (hx, hy) = g / 2 and S = zk + zm, D = zk - zm, the filtered recombination is
+            // (S.x hx + D.x hy, S.y hx + D.y hy) at e <= N/2 and (S.x hx - D.x hy, S.y hx - D.y hy)
+            // above: one packed product and one packed FMA (D negated exactly for the upper half)
+            const float2 S = cadd(zk, zm), D = lower ? csub(zk, zm) : csub(zm, zk);
+            float hx, hy;
+            f2unpack(f2mul(f2pack(g.x, g.y), f2pack(0.5f, 0.5f)), hx, hy);
+            const uint64_t ab = f2mul(f2pack(S.x, S.y), f2pack(hx, hx));
+            f2unpack(f2fma(f2pack(D.x, D.y), f2pack(hy, hy), ab), v[q].x, v[q].y);
         }
         dft<16, true>(v);
 #pragma unroll
