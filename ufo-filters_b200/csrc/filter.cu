@@ -629,19 +629,71 @@ __device__ __forceinline__ void fast_pass(const float2 *src, float2 *dst, const 
     }
 }
 
-// Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer,
-// which holds the transform in natural (unswizzled) order.
-template <int LOGN, bool INV>
-__device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 *tab2, const float2 *tab3,
-                                             uint32_t t, uint32_t T)
+// Lanes of this thread's group of G <= 32 threads (groups are aligned within the warp).
+template <uint32_t G>
+__device__ __forceinline__ uint32_t group_lanes()
 {
-    constexpr uint32_t N = 1u << LOGN;
+    if constexpr (G >= 32)
+        return 0xffffffffu;
+    else
+        return ((1u << G) - 1u) << ((threadIdx.x & 31u) & ~(G - 1u));
+}
+
+// Barrier of G threads (aligned, contiguous): the CTA barrier when G is the whole CTA, named
+// barrier `id` (1 .. 15: teams take 1 .. TEAMS, team pairs the ids after them) for several warps,
+// a warp-level barrier for one warp or part of one.  The teams of a CTA only meet where
+// they share data.
+template <uint32_t G>
+__device__ __forceinline__ void group_sync(uint32_t id)
+{
+    if constexpr (G >= kFastThreads)
+        __syncthreads();
+    else if constexpr (G > 32)
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(G) : "memory");
+    else
+        __syncwarp(group_lanes<G>());
+}
+
+// The same barrier, returning whether `pred` held in any of the G threads.
+template <uint32_t G>
+__device__ __forceinline__ bool group_sync_or(uint32_t id, bool pred)
+{
+    if constexpr (G >= kFastThreads) {
+        return __syncthreads_or(pred) != 0;
+    } else if constexpr (G > 32) {
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\t"
+            "selp.u32 %0, 1, 0, q;\n\t}"
+            : "=r"(r)
+            : "r"((uint32_t)pred), "r"(id), "n"(G)
+            : "memory");
+        return r != 0;
+    } else {
+        const uint32_t mask = group_lanes<G>();
+        __syncwarp(mask);
+        return __any_sync(mask, pred) != 0;
+    }
+}
+
+// Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer,
+// which holds the transform in natural (unswizzled) order.  The team synchronises between passes;
+// the barrier after the last pass spans LASTG threads (id `last_id`), so that a partner team can
+// read the result.
+template <int LOGN, bool INV, uint32_t LASTG>
+__device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 *tab2, const float2 *tab3,
+                                             uint32_t t, uint32_t team, uint32_t last_id)
+{
+    constexpr uint32_t N = 1u << LOGN, T = N / 16;
     constexpr int R3 = (int)(N / 256);
     fast_pass<16, INV, R3 == 1>(a, b, tab2, N, 16, t, T);
-    __syncthreads();
-    if (R3 == 1) return b;
+    if (R3 == 1) {
+        group_sync<LASTG>(last_id);
+        return b;
+    }
+    group_sync<T>(1 + team);
     fast_pass<(R3 > 1 ? R3 : 2), INV, true>(b, a, tab3, N, 256, t, T);
-    __syncthreads();
+    group_sync<LASTG>(last_id);
     return a;
 }
 
@@ -684,14 +736,18 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         if (mm.hasa) bulk_load_1d(stg, row_start(src, mm.ra, y, p), wl * 4u, &s_bar[team]);
         if (mm.hasb) bulk_load_1d(stg + N, row_start(src, mm.rb, y, p), wl * 4u, &s_bar[team]);
     };
-    if (STG) {
-        if (t == 0) {
-            mbar_init(&s_bar[team], 1);
-            fence_barrier_init();
-        }
-        __syncthreads();
-        if (t == 0 && iters > 0) issue(0);
+    if (STG && t == 0) {
+        mbar_init(&s_bar[team], 1);
+        fence_barrier_init();
     }
+    __syncthreads();  // tables, gains and barriers are ready; from here on the teams meet only in
+                      // pairs, where a quad output cell takes both teams' results
+    if (STG && t == 0 && iters > 0) issue(0);
+    // the cell store of the slice-quad output reads the partner team's result
+    constexpr bool CELLS = OUT == OUT_F16_QUADS && TEAMS % 2 == 0;
+    static_assert(2 * T <= 32 || TEAMS + TEAMS / 2 <= 15, "named barrier ids 1 .. 15");
+    constexpr uint32_t SG = CELLS ? 2 * T : T;  // threads that share a result buffer
+    const uint32_t sid = CELLS ? 1 + TEAMS + (team >> 1) : 1 + team;
     for (uint32_t it = 0; it < iters; it++) {
         const uint32_t pair = (it * gridDim.x + blockIdx.x) * TEAMS + team;
         const bool live = pair < npairs;
@@ -764,22 +820,25 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
                 }
             }
         }
-        // tables loaded; the previous item's output reads and this item's staged reads are done
+        // the previous item's output reads (the partner team's too, for quad cells) and this item's
+        // staged reads are done; teams that share buffers leave together on a failed wait
         if (STG) {
-            if (__syncthreads_or(failed)) {
-                if (threadIdx.x == 0) atomicExch(err, kErrTmaTimeout);
-                if (t == 0) mbar_wait_bounded(&s_bar[team], it & 1u, kWaitLimitNs);  // the copy in flight
+            if (group_sync_or<SG>(sid, failed)) {
+                if (t == 0) {
+                    atomicExch(err, kErrTmaTimeout);
+                    mbar_wait_bounded(&s_bar[team], it & 1u, kWaitLimitNs);  // the copy in flight
+                }
                 return;
             }
             if (t == 0 && it + 1 < iters) issue(it + 1);
         } else {
-            __syncthreads();
+            group_sync<SG>(sid);
         }
         dft<16, false>(v);
 #pragma unroll
         for (int q = 0; q < 16; q++) bufA[swz(t * 16 + q)] = v[q];
-        __syncthreads();
-        const float2 *Z = fast_tail<LOGN, false>(bufA, bufB, tab2, tab3, t, T);
+        group_sync<T>(1 + team);
+        const float2 *Z = fast_tail<LOGN, false, T>(bufA, bufB, tab2, tab3, t, team, 1 + team);
         float2 *O = (Z == bufA) ? bufB : bufA;
         // separate the two rows' spectra, apply the gains, recombine (element e = t + q N/16)
 #pragma unroll
@@ -801,8 +860,8 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         dft<16, true>(v);
 #pragma unroll
         for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
-        __syncthreads();
-        const float2 *X = fast_tail<LOGN, true>(O, O == bufA ? bufB : bufA, tab2, tab3, t, T);
+        group_sync<T>(1 + team);
+        const float2 *X = fast_tail<LOGN, true, SG>(O, O == bufA ? bufB : bufA, tab2, tab3, t, team, sid);
         if constexpr (OUT == OUT_F16_QUADS && TEAMS % 2 == 0) {
             // teams 2u and 2u + 1 hold the two halves (slices 4g, 4g+1 and 4g+2, 4g+3 at one angle)
             // of the same cells, and the barrier that ended the transform made both results visible:
