@@ -86,9 +86,8 @@ typedef enum {
                               pair_stride = round_up(crop_width + 1, 4) */
     UFOB_LAYOUT_QUADS = 2  /* F16 only, for a stack of sinograms: [ceil(nslices/4)][height][cells]
                               16-byte cells, cell j of group g holding the taps s[j-1], s[j] of
-                              slices 4g..4g+3 as halves (s0[j-1], s1[j-1], s0[j], s1[j],
-                              s2[j-1], s3[j-1], s2[j], s3[j]): each 8-byte half cell is one
-                              slice pair; cells >= crop_width + 1 */
+                              slices 4g..4g+3 as halves (s0[j-1], s1[j-1], s2[j-1], s3[j-1],
+                              s0[j], s1[j], s2[j], s3[j]); cells >= crop_width + 1 */
 } ufob_layout;
 
 typedef struct {

@@ -29,8 +29,7 @@ def test_filter_quad_cells(cuda, nz):
     ref = oracle.fft_filter_ifft(raw.reshape(-1, W), size_x=256, crop_width=W).reshape(nz, P, W)
     for z in range(4 * G):
         g, k = divmod(z, 4)
-        # halves (s0[j-1], s1[j-1], s0[j], s1[j], s2[j-1], s3[j-1], s2[j], s3[j])
-        lo, hi = h[g, :, :, 4 * (k // 2) + k % 2], h[g, :, :, 4 * (k // 2) + 2 + k % 2]
+        lo, hi = h[g, :, :, k], h[g, :, :, 4 + k]
         if z >= nz:
             assert np.all(lo == 0) and np.all(hi == 0)
             continue

@@ -554,8 +554,8 @@ __global__ void __launch_bounds__(256) k_bp_batch(const BatchBP *__restrict__ jo
 // Storage form SINO_F16_QUADS, written by the filter stage for a stack: cell
 // (g, p, j) of 16 bytes carries both interpolation taps of the four slices
 // 4g..4g+3 at angle p,
-//   word 0 = (s0[j-1], s1[j-1])   word 1 = (s0[j], s1[j])
-//   word 2 = (s2[j-1], s3[j-1])   word 3 = (s2[j], s3[j])
+//   word 0 = (s0[j-1], s1[j-1])   word 1 = (s2[j-1], s3[j-1])
+//   word 2 = (s0[j],   s1[j])     word 3 = (s2[j],   s3[j])
 // for j = 0..W (taps outside the row are 0).  One 128-bit shared load then
 // feeds four updates, so the per-update instruction count is dominated by the
 // FMAs themselves.  The TMA box is (4 words, window, 1 angle, ZT/4 groups);
@@ -772,15 +772,15 @@ __device__ __forceinline__ bool bp_tile_quads(const CUtensorMap *map, const BPAr
                             float *pz = &part[j][4 * q];
                             if (ACC == QACC_F32) {
                                 mix_fma2(pz[0], pz[1], v.x, wlo);
-                                mix_fma2(pz[0], pz[1], v.y, whi);
-                                mix_fma2(pz[2], pz[3], v.z, wlo);
+                                mix_fma2(pz[0], pz[1], v.z, whi);
+                                mix_fma2(pz[2], pz[3], v.y, wlo);
                                 mix_fma2(pz[2], pz[3], v.w, whi);
                             } else if (ACC == QACC_LERP) {
-                                mix_add2(pz[0], pz[1], h2_fma(v.y, whi, h2_mul(v.x, wlo)));
-                                mix_add2(pz[2], pz[3], h2_fma(v.w, whi, h2_mul(v.z, wlo)));
+                                mix_add2(pz[0], pz[1], h2_fma(v.z, whi, h2_mul(v.x, wlo)));
+                                mix_add2(pz[2], pz[3], h2_fma(v.w, whi, h2_mul(v.y, wlo)));
                             } else {
-                                hs[j][2 * q] = h2_fma(v.y, whi, h2_fma(v.x, wlo, hs[j][2 * q]));
-                                hs[j][2 * q + 1] = h2_fma(v.w, whi, h2_fma(v.z, wlo, hs[j][2 * q + 1]));
+                                hs[j][2 * q] = h2_fma(v.z, whi, h2_fma(v.x, wlo, hs[j][2 * q]));
+                                hs[j][2 * q + 1] = h2_fma(v.w, whi, h2_fma(v.y, wlo, hs[j][2 * q + 1]));
                             }
                         }
                     }

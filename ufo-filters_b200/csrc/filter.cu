@@ -383,14 +383,15 @@ __device__ __forceinline__ void store_pair(const PairMap &m, GET X, void *__rest
                                            uint32_t out_pitch, uint32_t t0, uint32_t step)
 {
     if (OUT == OUT_F16_QUADS) {
-        // half cell `half` of cell j: the words of taps j-1 and j, rows a, b in the low, high halves
-        uint2 *o = reinterpret_cast<uint2 *>(out) + m.cell0 * 2 + m.half;
+        // words `half` (taps j-1) and 2 + `half` (taps j) of cell j; rows a, b in the low, high halves
+        uint32_t *o = reinterpret_cast<uint32_t *>(out) + m.cell0 * 4;
         for (uint32_t j = t0; j < out_pitch; j += step) {
             float2 lo = (j >= 1 && j - 1 < out_w) ? X(j - 1) : make_float2(0.f, 0.f);
             float2 hi = (j < out_w) ? X(j) : make_float2(0.f, 0.f);
             if (!m.hasa) lo.x = hi.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
             if (!m.hasb) lo.y = hi.y = 0.f;
-            o[(size_t)j * 2] = make_uint2(pack_pair<OUT>(lo.x, lo.y), pack_pair<OUT>(hi.x, hi.y));
+            o[(size_t)j * 4 + m.half] = pack_pair<OUT>(lo.x, lo.y);
+            o[(size_t)j * 4 + 2 + m.half] = pack_pair<OUT>(hi.x, hi.y);
         }
     } else if (OUT == OUT_F16_PAIRS || OUT == OUT_BF16_PAIRS) {
         uint32_t *o = reinterpret_cast<uint32_t *>(out);
@@ -639,8 +640,9 @@ __device__ __forceinline__ uint32_t group_lanes()
 }
 
 // Barrier of G threads (aligned, contiguous): the CTA barrier when G is the whole CTA, named
-// barrier `id` (team t takes 1 + t) for several warps, a warp-level barrier for one warp or part
-// of one.  The teams of a CTA share only the read-only tables, so they never wait for each other.
+// barrier `id` (1 .. 15: teams take 1 .. TEAMS, team pairs the ids after them) for several warps,
+// a warp-level barrier for one warp or part of one.  The teams of a CTA only meet where
+// they share data.
 template <uint32_t G>
 __device__ __forceinline__ void group_sync(uint32_t id)
 {
@@ -676,7 +678,8 @@ __device__ __forceinline__ bool group_sync_or(uint32_t id, bool pred)
 
 // Passes 2 and 3 (Ns = 16, 256) of an N-point transform, src -> ... ; returns the result buffer,
 // which holds the transform in natural (unswizzled) order.  The team synchronises between passes;
-// the barrier after the last pass spans LASTG threads (id `last_id`).
+// the barrier after the last pass spans LASTG threads (id `last_id`), so that a partner team can
+// read the result.
 template <int LOGN, bool INV, uint32_t LASTG>
 __device__ __forceinline__ float2 *fast_tail(float2 *a, float2 *b, const float2 *tab2, const float2 *tab3,
                                              uint32_t t, uint32_t team, uint32_t last_id)
@@ -737,9 +740,14 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         mbar_init(&s_bar[team], 1);
         fence_barrier_init();
     }
-    __syncthreads();  // tables, gains and barriers are ready; from here on each team runs alone
+    __syncthreads();  // tables, gains and barriers are ready; from here on the teams meet only in
+                      // pairs, where a quad output cell takes both teams' results
     if (STG && t == 0 && iters > 0) issue(0);
-    static_assert(T <= 32 || TEAMS <= 15, "named barrier ids 1 .. 15");
+    // the cell store of the slice-quad output reads the partner team's result
+    constexpr bool CELLS = OUT == OUT_F16_QUADS && TEAMS % 2 == 0;
+    static_assert(2 * T <= 32 || TEAMS + TEAMS / 2 <= 15, "named barrier ids 1 .. 15");
+    constexpr uint32_t SG = CELLS ? 2 * T : T;  // threads that share a result buffer
+    const uint32_t sid = CELLS ? 1 + TEAMS + (team >> 1) : 1 + team;
     for (uint32_t it = 0; it < iters; it++) {
         const uint32_t pair = (it * gridDim.x + blockIdx.x) * TEAMS + team;
         const bool live = pair < npairs;
@@ -812,10 +820,10 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
                 }
             }
         }
-        // the team's output reads of the previous item and its staged reads of this one are done;
-        // the team leaves together on a failed wait
+        // the previous item's output reads (the partner team's too, for quad cells) and this item's
+        // staged reads are done; teams that share buffers leave together on a failed wait
         if (STG) {
-            if (group_sync_or<T>(1 + team, failed)) {
+            if (group_sync_or<SG>(sid, failed)) {
                 if (t == 0) {
                     atomicExch(err, kErrTmaTimeout);
                     mbar_wait_bounded(&s_bar[team], it & 1u, kWaitLimitNs);  // the copy in flight
@@ -824,7 +832,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
             }
             if (t == 0 && it + 1 < iters) issue(it + 1);
         } else {
-            group_sync<T>(1 + team);
+            group_sync<SG>(sid);
         }
         dft<16, false>(v);
 #pragma unroll
@@ -853,8 +861,34 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
 #pragma unroll
         for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
         group_sync<T>(1 + team);
-        const float2 *X = fast_tail<LOGN, true, T>(O, O == bufA ? bufB : bufA, tab2, tab3, t, team, 1 + team);
-        if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, t, T);
+        const float2 *X = fast_tail<LOGN, true, SG>(O, O == bufA ? bufB : bufA, tab2, tab3, t, team, sid);
+        if constexpr (OUT == OUT_F16_QUADS && TEAMS % 2 == 0) {
+            // teams 2u and 2u + 1 hold the two halves (slices 4g, 4g+1 and 4g+2, 4g+3 at one angle)
+            // of the same cells, and the barrier that ended the transform made both results visible:
+            // the pair's 2T threads write whole 16-byte cells, consecutive across threads
+            if (live) {
+                const uint32_t u = team >> 1, i0 = threadIdx.x - u * 2 * T;
+                const uint32_t pair0 = pair - (team & 1u);
+                const PairMap m0 = map_pair<OUT>(pair0, rows, P, out_pitch);
+                const PairMap m1 = map_pair<OUT>(pair0 + 1, rows, P, out_pitch);
+                const size_t xoff = (size_t)(X - bufA);  // this team's result: bufA or bufB
+                const float2 *X0 = gains + (N / 2 + 2) + (size_t)(2 * u) * 2 * N + xoff;
+                const float2 *X1 = X0 + 2 * N;
+                uint4 *o = reinterpret_cast<uint4 *>(out) + m0.cell0;
+                auto taps = [&](const float2 *Xh, const PairMap &mh, uint32_t j, bool prev) {
+                    const uint32_t e = prev ? j - 1 : j;
+                    float2 v = ((!prev || j >= 1) && e < out_w) ? Xh[e] : make_float2(0.f, 0.f);
+                    if (!mh.hasa) v.x = 0.f;  // slices past the stack: exact zeros, not FFT round-off
+                    if (!mh.hasb) v.y = 0.f;
+                    return pack_pair<OUT>(v.x, v.y);
+                };
+                for (uint32_t j = i0; j < out_pitch; j += 2 * T)
+                    o[j] = make_uint4(taps(X0, m0, j, true), taps(X1, m1, j, true), taps(X0, m0, j, false),
+                                      taps(X1, m1, j, false));
+            }
+        } else {
+            if (live) store_pair<OUT>(m, [X](uint32_t i) { return X[i]; }, out, out_w, out_pitch, t, T);
+        }
     }
 }
 

@@ -31,8 +31,7 @@ namespace ufob {
 
 // ------------------------------------------------------------ FP32 stack -> slice-quad cells
 
-// cell (g, p, j), j <= W: halves (s0[j-1], s1[j-1], s0[j], s1[j], s2[j-1], s3[j-1], s2[j], s3[j]) of
-// slices 4g..4g+3
+// cell (g, p, j), j <= W: halves (s0[j-1], s1[j-1], s2[j-1], s3[j-1], s0[j], .., s3[j]) of slices 4g..4g+3
 __global__ void k_pack_quads(const float *__restrict__ in, uint32_t W, uint32_t P, uint32_t Z, uint32_t groups,
                              uint4 *__restrict__ out)
 {
@@ -49,8 +48,8 @@ __global__ void k_pack_quads(const float *__restrict__ in, uint32_t W, uint32_t 
             lo[k] = (z < Z && j >= 1) ? __ldg(row + j - 1) : 0.f;
             hi[k] = (z < Z && j < W) ? __ldg(row + j) : 0.f;
         }
-        __half2 w0 = __floats2half2_rn(lo[0], lo[1]), w1 = __floats2half2_rn(hi[0], hi[1]);
-        __half2 w2 = __floats2half2_rn(lo[2], lo[3]), w3 = __floats2half2_rn(hi[2], hi[3]);
+        __half2 w0 = __floats2half2_rn(lo[0], lo[1]), w1 = __floats2half2_rn(lo[2], lo[3]);
+        __half2 w2 = __floats2half2_rn(hi[0], hi[1]), w3 = __floats2half2_rn(hi[2], hi[3]);
         out[c] = make_uint4(*reinterpret_cast<uint32_t *>(&w0), *reinterpret_cast<uint32_t *>(&w1),
                             *reinterpret_cast<uint32_t *>(&w2), *reinterpret_cast<uint32_t *>(&w3));
     }
