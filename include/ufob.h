@@ -148,8 +148,8 @@ typedef struct {
     uint32_t roi_width;       /* "roi-width", 0 = sinogram width */
     uint32_t roi_height;      /* "roi-height", 0 = sinogram width */
     /* engine extensions */
-    int compensated;          /* blocked Kahan over angle blocks: 0 off, 1 on, -1 auto (>=1500 angles
-                                 when the sinogram is stored as F16/BF16) */
+    int compensated;          /* blocked Kahan over angle blocks: 1 on; 0 or -1 (default) off, since
+                                 16-bit storage rounding outweighs the FP32 block sums' error */
     int tile;                 /* kernel shape id from the autotuner, -1 = automatic */
     int half_sums;            /* F16 QUADS sinograms only: 0 (default) every product accumulated in
                                  FP32; 1 interpolation and sums over blocks of 8 angles in packed
