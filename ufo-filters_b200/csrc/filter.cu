@@ -862,7 +862,7 @@ __global__ void __launch_bounds__(kFastThreads, 2) k_filter_fast(const RowSource
         for (int q = 0; q < 16; q++) O[swz(t * 16 + q)] = v[q];
         group_sync<T>(1 + team);
         const float2 *X = fast_tail<LOGN, true, SG>(O, O == bufA ? bufB : bufA, tab2, tab3, t, team, sid);
-        if constexpr (OUT == OUT_F16_QUADS && TEAMS % 2 == 0) {
+        if constexpr (CELLS) {
             // teams 2u and 2u + 1 hold the two halves (slices 4g, 4g+1 and 4g+2, 4g+3 at one angle)
             // of the same cells, and the barrier that ended the transform made both results visible:
             // the pair's 2T threads write whole 16-byte cells, consecutive across threads
