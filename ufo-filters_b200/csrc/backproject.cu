@@ -1096,8 +1096,20 @@ ufob_status bp_quads_launch(const BPGeometry &g, const void *d_sino, uint32_t pi
     if ((uintptr_t)d_sino & 15) return fail(UFOB_ERR_INVALID, "backproject: slice-quad base must be 16-byte aligned");
     if (pitch < g.W + 1 || group_pitch < (uint64_t)pitch * g.P)
         return fail(UFOB_ERR_INVALID, "backproject: slice-quad pitches too small");
-    // measured on B200 (2048^2 x 1500, 32 slices): 32x16 px x 16 slices, 2 stages of 16 angles is fastest
-    if (tile < 0) tile = g.nz <= 4 ? 0 : (g.nz <= 8 ? 2 : 8);
+    // Measured on B200 (2048^2 x 1500): with compensated block sums 32x16 px x 16 slices, 2 stages of
+    // 16 angles (tile 8) is fastest; with FP32 block sums 32x8 px x 32 slices, 2 stages of 8 angles
+    // (tile 11: each coordinate serves 32 slices) ran at 6644 against 6482 GUPS, so it is taken
+    // unless rounding the stack up to 32 slices costs more than that.
+    if (tile < 0) {
+        if (g.nz <= 4) {
+            tile = 0;
+        } else if (g.nz <= 8) {
+            tile = 2;
+        } else {
+            const uint64_t w32 = (g.nz + 31) / 32 * 32, w16 = (g.nz + 15) / 16 * 16;
+            tile = !kahan && w32 * 6482 <= w16 * 6644 ? 11 : 8;
+        }
+    }
     switch (acc) {
     case QACC_F32:
         return kahan ? quads_tile<QACC_F32, true>(tile, g, d_sino, pitch, group_pitch, d_out, stream)
