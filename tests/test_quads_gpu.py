@@ -17,16 +17,19 @@ def _raw(nz, P, W, seed):
     return np.random.default_rng(seed).standard_normal((nz, P, W)).astype(np.float32)
 
 
+# every FFT size of the register-radix filter: its teams meet as half warps (256), on named
+# barriers (512, 1024), or as the whole CTA (2048), and one team fills a CTA alone (4096)
+@pytest.mark.parametrize("W,N", [(250, 256), (500, 512), (1000, 1024), (2000, 2048), (4000, 4096)])
 @pytest.mark.parametrize("nz", [1, 4, 6])
-def test_filter_quad_cells(cuda, nz):
-    W, P = 250, 7
+def test_filter_quad_cells(cuda, nz, W, N):
+    P = 7
     raw = _raw(nz, P, W, 3)
-    f = ufob.FilterTask(size_x=256, crop_width=W)
+    f = ufob.FilterTask(size_x=N, crop_width=W)
     q = f.process(torch.from_numpy(raw).cuda(), dtype=ufob.F16, layout=ufob.QUADS)
     G = (nz + 3) // 4
     assert q.shape == (G, P, W + 1, 4)
     h = q.cpu().view(torch.int32).numpy().view(np.float16).astype(np.float32).reshape(G, P, W + 1, 8)
-    ref = oracle.fft_filter_ifft(raw.reshape(-1, W), size_x=256, crop_width=W).reshape(nz, P, W)
+    ref = oracle.fft_filter_ifft(raw.reshape(-1, W), size_x=N, crop_width=W).reshape(nz, P, W)
     for z in range(4 * G):
         g, k = divmod(z, 4)
         lo, hi = h[g, :, :, k], h[g, :, :, 4 + k]
@@ -37,9 +40,12 @@ def test_filter_quad_cells(cuda, nz):
         assert oracle.rel_l2(hi[:, :W], ref[z]) < 2e-3
         assert oracle.rel_l2(lo[:, 1:], ref[z]) < 2e-3
         assert np.all(lo[:, 0] == 0) and np.all(hi[:, W] == 0)
-        # the halves are the FP16 rounding of the rows form (the FFT pairs other rows: rounding may differ)
+        # the halves are the FP16 rounding of the rows form: the FFT pairs other rows, so the FP32
+        # round-off of the two transforms (growing with N) may move a value by one FP16 step, which
+        # for small values is one step of the row's largest value
         rows = f.process(torch.from_numpy(raw[z]).cuda(), dtype=ufob.F16).float().cpu().numpy()
-        assert np.all(np.abs(hi[:, :W] - rows) <= 2.0 ** -10 * np.abs(rows) + 1e-7)
+        scale = float(np.abs(rows).max())
+        assert np.all(np.abs(hi[:, :W] - rows) <= 2.0 ** -10 * np.abs(rows) + 2.0 ** -11 * scale)
         assert np.mean(hi[:, :W] == rows) > 0.9
 
 
