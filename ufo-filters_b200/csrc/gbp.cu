@@ -883,6 +883,12 @@ static ufob_status launch_gbp_col(GBPColArgs c, bool cone, bool *launched, cudaS
         *launched = true;
         return cone ? launch_gbp_col_t<true, 4, 3>(c, s) : launch_gbp_col_t<false, 4, 3>(c, s);
     }
+    // a third stage of 3 projections beats 2 stages of 4 (configuration-2 cone: 950 against 915
+    // GUPS; 2 projections per stage, 4 or 5 stages: 876 / 880)
+    if (GBPColSmem<3, 3>::bytes(c.slot_floats) <= kBudget) {
+        *launched = true;
+        return cone ? launch_gbp_col_t<true, 3, 3>(c, s) : launch_gbp_col_t<false, 3, 3>(c, s);
+    }
     if (GBPColSmem<4, 2>::bytes(c.slot_floats) <= kBudget) {
         *launched = true;
         return cone ? launch_gbp_col_t<true, 4, 2>(c, s) : launch_gbp_col_t<false, 4, 2>(c, s);
