@@ -875,6 +875,11 @@ static ufob_status launch_gbp_col(GBPColArgs c, bool cone, bool *launched, cudaS
         *launched = true;
         return cone ? launch_gbp_col_t<true, 8, 3>(c, s) : launch_gbp_col_t<false, 8, 3>(c, s);
     }
+    // three stages of 6 before two of 8 (configuration-2 laminography: 1055 against 1013 GUPS)
+    if (GBPColSmem<6, 3>::bytes(c.slot_floats) <= kBudget) {
+        *launched = true;
+        return cone ? launch_gbp_col_t<true, 6, 3>(c, s) : launch_gbp_col_t<false, 6, 3>(c, s);
+    }
     if (GBPColSmem<8, 2>::bytes(c.slot_floats) <= kBudget) {
         *launched = true;
         return cone ? launch_gbp_col_t<true, 8, 2>(c, s) : launch_gbp_col_t<false, 8, 2>(c, s);
