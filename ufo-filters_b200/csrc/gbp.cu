@@ -1001,6 +1001,7 @@ struct ufob_gbp {
     GBPColPlan col_plan;
     // device state
     DevBuf d_geom, d_zvals, d_tab_f, d_tab_d, d_proj, d_vol, d_proj16;
+    DevBuf d_proj_h;  // compute-type half on the staged kernel: the projections rounded to FP16, as FP32
     uint32_t pushed = 0, pw = 0, ph = 0;
     bool volume_ready = false;
     // texture objects over the projections of the last call (rebuilt when base/shape/mode change)
@@ -1033,6 +1034,20 @@ __global__ void k_proj_to_half(const float *__restrict__ in, uint32_t W, uint32_
         const uint64_t r = i / W;
         const uint32_t y = (uint32_t)(r % H), p = (uint32_t)(r / H);
         out[(size_t)p * plane + (size_t)y * pitch + x] = __float2half_rn(__ldg(in + i));
+    }
+}
+
+// The projections rounded to FP16 and widened back to FP32 (both conversions exact for the values
+// kept), four per thread: the very samples the FP16 gathers of compute-type half read.
+__global__ void k_proj_round_half(const float4 *__restrict__ in, uint64_t n4, float4 *__restrict__ out)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
+        float4 v = __ldg(in + i);
+        v.x = __half2float(__float2half_rn(v.x));
+        v.y = __half2float(__float2half_rn(v.y));
+        v.z = __half2float(__float2half_rn(v.z));
+        v.w = __half2float(__float2half_rn(v.w));
+        out[i] = v;
     }
 }
 
@@ -1356,8 +1371,9 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
                     : launch_gbp_rt<false, double>(a, g->result_type, paramz, s);
     }
     a.tab = g->d_tab_f.ptr;
-    if (g->compute_type == 0 && !g->interpolation && g->staging && g->result_type == RT_FLOAT &&
-        g->store_type == ST_FLOAT && paramz && a.addr == AD_CLAMP && W % 4 == 0 && !((uintptr_t)d_proj & 15)) {
+    if ((g->compute_type == 0 || g->compute_type == 2) && !g->interpolation && g->staging &&
+        g->result_type == RT_FLOAT && g->store_type == ST_FLOAT && paramz && a.addr == AD_CLAMP && W % 4 == 0 &&
+        !((uintptr_t)d_proj & 15)) {
         // TMA-staged detector windows for geometries whose u does not depend on z; the plan (host
         // FP64 tables, window size) is kept while the geometry stays the same
         std::vector<double> key(table);
@@ -1371,8 +1387,23 @@ static ufob_status gbp_compute(ufob_gbp *g, const float *d_proj, uint32_t W, uin
             g->col_key.swap(key);
         }
         if (g->col_plan.ok) {
+            const float *src = d_proj;
+            if (g->compute_type == 2) {
+                // compute-type half: FP16 samples with FP32 coordinates, weights and sums, the
+                // arithmetic of the FP16 gathers, staged from a rounded FP32 copy
+                const uint64_t n4 = (uint64_t)n * H * W / 4;
+                UFOB_TRY(g->d_proj_h.ensure(n4 * 16));
+                if (n4) {
+                    const uint32_t grid = (uint32_t)std::min<uint64_t>((n4 + 255) / 256, (uint64_t)num_sms() * 16);
+                    k_proj_round_half<<<grid, 256, 0, s>>>(reinterpret_cast<const float4 *>(d_proj), n4,
+                                                           g->d_proj_h.as<float4>());
+                    UFOB_CUDA_TRY(cudaGetLastError());
+                    note_launch();
+                }
+                src = g->d_proj_h.as<float>();
+            }
             GBPColArgs c;
-            c.proj = d_proj;
+            c.proj = src;
             c.tab = g->d_tab_f.as<float>();
             c.zvals = a.zvals;
             c.W = W;
