@@ -263,13 +263,14 @@ ufob_status ufob_gbp_set_property(ufob_gbp *g, const char *name, double value);
 /* String properties as the reference's enums (parameter, compute-type, result-type, store-type,
  * addressing-mode), plus the engine property "interpolation": "exact" (default, FP32 weights)
  * or "texture" (the texture unit's linear filter with 8-bit weights, as the reference samples
- * on a GPU; FP32 compute type).  compute-type "half" stores the projection samples as FP16
- * (texture gathers of 16-bit texels run at twice the FP32 rate) and keeps coordinates, weights
- * and sums in FP32; the reference's half type also computes those in half precision.  The
- * engine property "staging": "auto" (default) stages each projection's detector window in
- * shared memory by TMA where the geometry lets a z-column of voxels share its detector column
- * (float compute/result/store types, exact weights, parameter z, clamp addressing, width a
- * multiple of 4), else samples through texture gathers; "texture" always uses the gathers.
+ * on a GPU; FP32 compute type).  compute-type "half" rounds the projection samples to FP16
+ * and keeps coordinates, weights and sums in FP32 (staged from a rounded FP32 copy where staging
+ * applies, else through texture gathers of 16-bit texels); the reference's half type also
+ * computes those in half precision.  The engine property "staging": "auto" (default) stages
+ * each projection's detector window in shared memory by TMA where the geometry lets a z-column
+ * of voxels share its detector column (float or half compute, float result/store types, exact
+ * weights, parameter z, clamp addressing, width a multiple of 4), else samples through texture
+ * gathers; "texture" always uses the gathers.
  * Both give the same values to FP32 rounding. */
 ufob_status ufob_gbp_set_property_string(ufob_gbp *g, const char *name, const char *value);
 ufob_status ufob_gbp_set_array(ufob_gbp *g, const char *name, const double *values, uint32_t n);
